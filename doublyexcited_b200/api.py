@@ -1,0 +1,197 @@
+"""Python mirror of the reference's operator / eigensolver interface over the
+C ABI.  Arrays are numpy complex128 in the reference layout: a two-electron
+vector is X(1:M, 1:M) flattened column-major (electron 1 fastest); a block
+is shape (D, nev) in Fortran order."""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import check, de_complex, de_gmres, de_input, de_params, de_stats, lib
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _block(x: np.ndarray, dim: int) -> np.ndarray:
+    x = np.asarray(x)
+    if x.ndim == 1:
+        x = x.reshape(-1, 1)
+    x = np.asfortranarray(x, dtype=np.complex128)
+    if x.shape[0] != dim:
+        raise ValueError(f"vector length {x.shape[0]} != {dim}")
+    return x
+
+
+@dataclass
+class GplmrResult:
+    e: np.ndarray
+    x: np.ndarray
+    iterations: int
+    converged: bool
+    matvecs: int
+    matvecs_reference: int
+    max_residual: float
+    t_total_s: float
+    t_matvec_s: float
+    t_prec_s: float
+    t_dense_s: float
+
+
+class Problem:
+    """One operator instance (HAMILTONIAN + PARAMETERS of the reference) on
+    one GPU.  Mirrors ``INIT_STRUCTS``/``INIT_HAMILTONIAN``."""
+
+    def __init__(self, n: int, delta: float = 2.0, theta: float = 0.2, charge: float = 2.0,
+                 nelec: int = 2, nsmall: int = 22, tfactor: int = 4, device: int = 0,
+                 autodelta: bool = False, radius: float = 7.0):
+        L = lib()
+        p = de_params()
+        L.de_params_default(ctypes.byref(p))
+        p.n, p.delta, p.theta, p.charge = n, delta, theta, charge
+        p.nelec, p.nsmall, p.tfactor, p.device = nelec, nsmall, tfactor, device
+        p.autodelta, p.radius = int(bool(autodelta)), radius
+        h = ctypes.c_void_p()
+        check(L.de_problem_create(ctypes.byref(p), ctypes.byref(h)), "de_problem_create")
+        self._h = h
+        nn = ctypes.c_int()
+        m = ctypes.c_int64()
+        dim = ctypes.c_int64()
+        check(L.de_problem_dims(h, ctypes.byref(nn), ctypes.byref(m), ctypes.byref(dim)), "de_problem_dims")
+        self.nn, self.m, self.dim = nn.value, m.value, dim.value
+        self.n, self.nelec = n, nelec
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().de_problem_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def set_stream(self, cuda_stream: int) -> None:
+        """Run the handle's kernels on a caller's cudaStream_t, e.g.
+        ``torch.cuda.current_stream().cuda_stream`` (0 is the legacy default
+        stream)."""
+        check(lib().de_set_stream(self._h, ctypes.c_void_p(cuda_stream)), "de_set_stream")
+
+    # -- operator ---------------------------------------------------------
+    def hammult(self, x: np.ndarray) -> np.ndarray:
+        x = _block(x, self.dim)[:, 0].copy()
+        y = np.empty_like(x)
+        check(lib().de_hammult(self._h, _ptr(x), _ptr(y), self.dim), "de_hammult")
+        return y
+
+    def matblock(self, x: np.ndarray) -> np.ndarray:
+        x = _block(x, self.dim)
+        y = np.empty_like(x)
+        check(lib().de_matblock(self._h, _ptr(x), _ptr(y), self.m, self.dim // self.m, x.shape[1]),
+              "de_matblock")
+        return y
+
+    def matblock_d(self, x_ptr: int, y_ptr: int, nev: int) -> None:
+        """Device-pointer MATBLOCK (e.g. torch tensors' data_ptr())."""
+        check(lib().de_matblock_d(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), self.m,
+                                  self.dim // self.m, nev), "de_matblock_d")
+
+    def dots(self, bras: np.ndarray, kets: np.ndarray, hermitian: bool = True) -> np.ndarray:
+        b = _block(bras, bras.shape[0])
+        k = _block(kets, b.shape[0])
+        out = np.empty((b.shape[1], k.shape[1]), np.complex128, order="F")
+        check(lib().de_dots(self._h, _ptr(b), _ptr(k), b.shape[0], b.shape[1], k.shape[1], _ptr(out),
+                            int(hermitian)), "de_dots")
+        return out
+
+    def get_expects(self, psi: np.ndarray, cshiftopt: bool = False) -> np.ndarray:
+        psi = _block(psi, self.dim)
+        out = np.empty(psi.shape[1], np.complex128)
+        check(lib().de_get_expects(self._h, _ptr(psi), psi.shape[1], int(cshiftopt), _ptr(out)),
+              "de_get_expects")
+        return out
+
+    # -- eigensolver ----------------------------------------------------------
+    def gplmr_eig(self, x0: np.ndarray, sigma: complex, ns: int = 5, maxit: int = 100, tol: float = 1e-7,
+                  max_inner_iter: int = 5, usepetscflag: int = 1, compat_first_column_only: bool = False,
+                  outmodulus: int = 0) -> GplmrResult:
+        x = _block(x0, self.dim).copy(order="F")
+        nev = x.shape[1]
+        e = np.empty(nev, np.complex128)
+        gm = de_gmres(max_inner_iter, usepetscflag, 1e-3, int(bool(compat_first_column_only)))
+        st = de_stats()
+        check(lib().de_gplmr_eig(self._h, _ptr(x), _ptr(e), self.m, self.dim // self.m,
+                                 de_complex(complex(sigma).real, complex(sigma).imag), nev, ns, maxit, tol,
+                                 ctypes.byref(gm), outmodulus, ctypes.byref(st)), "de_gplmr_eig")
+        return GplmrResult(e, x, st.iterations, bool(st.converged), st.matvecs, st.matvecs_reference,
+                           st.max_residual, st.t_total_s, st.t_matvec_s, st.t_prec_s, st.t_dense_s)
+
+
+# -- configuration ---------------------------------------------------------------
+
+def read_input(path: str | None, argv: list[str] | None = None) -> dict:
+    """Input.Inp namelists + command-line keys (get_input / get_args)."""
+    L = lib()
+    inp = de_input()
+    L.de_input_default(ctypes.byref(inp))
+    args = [a.encode() for a in (argv or [])]
+    arr = (ctypes.c_char_p * max(1, len(args)))(*args)
+    check(L.de_read_input(path.encode() if path else None, len(args), arr, ctypes.byref(inp)),
+          "de_read_input")
+    p = inp.params
+    return {
+        "N": p.n, "DELTA": p.delta, "RADIUS": p.radius, "AUTODELTA": bool(p.autodelta), "THETA": p.theta,
+        "CHARGE": p.charge, "NSMALL": p.nsmall, "TFACTOR": p.tfactor,
+        "GM_MAX_INNER_ITER": inp.gmres.max_inner_iter, "GM_USEPETSCFLAG": inp.gmres.usepetscflag,
+        "GM_TOL": inp.gmres.tol, "WRITEVECS": bool(inp.writevecs), "READVECS": bool(inp.readvecs),
+        "INVECFILE": inp.invecfile.decode(), "OUTVECFILE": inp.outvecfile.decode(),
+        "NUMORBS": inp.numorbs, "SINGLET": bool(inp.singlet), "NUMSKIP": inp.numskip,
+        "OUTMODULUS": inp.outmodulus, "TAKEREALPART": bool(inp.takerealpart), "HERMOPT": bool(inp.hermopt),
+        "CSHIFTOPT": bool(inp.cshiftopt), "GPLMR_NEV": inp.gplmr_nev, "GPLMR_NS": inp.gplmr_ns,
+        "GPLMR_MAXIT": inp.gplmr_maxit, "GPLMR_TOL": inp.gplmr_tol,
+        "GPLMR_SHIFT": complex(inp.gplmr_shift.re, inp.gplmr_shift.im),
+        "KDIM": inp.kdim, "LANBLOCKSIZE": inp.lanblocksize, "CHECK": inp.check, "LANTOL": inp.lantol,
+    }
+
+
+def input_file_arg(argv: list[str]) -> str:
+    L = lib()
+    args = [a.encode() for a in argv]
+    arr = (ctypes.c_char_p * max(1, len(args)))(*args)
+    buf = ctypes.create_string_buffer(512)
+    check(L.de_input_file_arg(len(args), arr, buf, 512), "de_input_file_arg")
+    return buf.value.decode()
+
+
+# -- eigenvector files ---------------------------------------------------------------
+
+def write_vectors(path: str, psi: np.ndarray, m: int) -> None:
+    psi = _block(psi, m * m)
+    check(lib().de_write_vectors(path.encode(), m, psi.shape[1], _ptr(psi)), "de_write_vectors")
+
+
+def read_vectors(path: str, m: int, num: int) -> np.ndarray:
+    out = np.empty((m * m, num), np.complex128, order="F")
+    check(lib().de_read_vectors(path.encode(), m, num, _ptr(out)), "de_read_vectors")
+    return out
+
+
+def vectors_header(path: str) -> tuple[int, int]:
+    m = ctypes.c_int64()
+    n = ctypes.c_int()
+    check(lib().de_vectors_header(path.encode(), ctypes.byref(m), ctypes.byref(n)), "de_vectors_header")
+    return m.value, n.value

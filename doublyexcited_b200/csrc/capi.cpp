@@ -1,0 +1,347 @@
+// capi.cpp -- C-ABI entry points: handle life cycle, HAMMULT / MATBLOCK /
+// dot products / expectations.  The eigensolver lives in gplmr.cpp, the
+// Input.Inp reader in input.cpp and the eigenvector files in vecio.cpp.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <tuple>
+
+#include "de_internal.h"
+
+namespace de {
+const char *last_error_str();
+}
+
+using namespace de;
+
+extern "C" {
+
+DE_API const char *de_version(void) { return "doublyexcited-b200 0.1 (sm_100a, FP64)"; }
+
+DE_API const char *de_last_error(void) { return last_error_str(); }
+
+DE_API const char *de_strerror(int s)
+{
+    switch (s) {
+    case DE_OK: return "ok";
+    case DE_E_INVALID: return "invalid argument";
+    case DE_E_SIZE: return "size mismatch";
+    case DE_E_CUDA: return "CUDA error";
+    case DE_E_NOMEM: return "out of memory";
+    case DE_E_UNSUPPORTED: return "unsupported option";
+    case DE_E_CHOLESKY: return "Cholesky breakdown";
+    case DE_E_GEVP: return "projected eigenproblem failed";
+    case DE_E_SVD: return "SVD failed";
+    case DE_E_ORTHO: return "inner-solve orthonormality check failed";
+    case DE_E_NOT_CONVERGED: return "not converged";
+    case DE_E_IO: return "I/O error";
+    case DE_E_PARSE: return "parse error";
+    case DE_E_LAPACK: return "host LAPACK not found";
+    case DE_E_NAN: return "non-finite value";
+    case DE_E_BUSY: return "admission refused";
+    default: return "unknown status";
+    }
+}
+
+DE_API void de_params_default(de_params *p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->n = 2;
+    p->delta = 0.5;
+    p->radius = 7.0;
+    p->autodelta = 1;
+    p->theta = 0.0;
+    p->charge = 2.0;
+    p->nelec = 2;
+    p->nsmall = 22;
+    p->tfactor = 4;
+    p->precision = DE_PREC_FP64;
+    p->device = 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- tables
+
+namespace {
+
+struct TinvKey {
+    int nout, nbig, nsmall;
+    double delta;
+    bool operator<(const TinvKey &o) const
+    {
+        return std::tie(nout, nbig, nsmall, delta) < std::tie(o.nout, o.nbig, o.nsmall, o.delta);
+    }
+};
+
+std::mutex g_tinv_mu;
+std::map<TinvKey, std::shared_ptr<std::vector<double>>> g_tinv;
+
+std::shared_ptr<std::vector<double>> cached_tinv(int nout, int nbig, int nsmall, double delta)
+{
+    std::lock_guard<std::mutex> lk(g_tinv_mu);
+    TinvKey k{nout, nbig, nsmall, delta};
+    auto it = g_tinv.find(k);
+    if (it != g_tinv.end()) return it->second;
+    auto v = std::make_shared<std::vector<double>>(getinverse(nout, nbig, nsmall, delta));
+    g_tinv[k] = v;
+    return v;
+}
+
+}  // namespace
+
+int de_problem::ensure_stage(int64_t elems)
+{
+    if (elems <= stage_elems) return DE_OK;
+    if (d_x) cudaFree(d_x);
+    if (d_y) cudaFree(d_y);
+    d_x = d_y = nullptr;
+    stage_elems = 0;
+    DE_CUDA(cudaMalloc(&d_x, elems * sizeof(double2)));
+    DE_CUDA(cudaMalloc(&d_y, elems * sizeof(double2)));
+    stage_elems = elems;
+    return DE_OK;
+}
+
+int de_problem::ensure_work(int64_t elems)
+{
+    if (elems <= work_elems) return DE_OK;
+    if (d_work) cudaFree(d_work);
+    d_work = nullptr;
+    work_elems = 0;
+    DE_CUDA(cudaMalloc(&d_work, elems * sizeof(double2)));
+    work_elems = elems;
+    return DE_OK;
+}
+
+int de_problem::matblock(const double2 *x, double2 *y, int nvec)
+{
+    cudaError_t e = (p.nelec == 2) ? hammult_launch(ham, x, y, nvec, dim, stream)
+                                   : hammult1_launch(ham, d_t1a, x, y, nvec, dim, stream);
+    if (e != cudaSuccess) return cuda_error(e, "hammult");
+    return DE_OK;
+}
+
+extern "C" {
+
+DE_API int de_problem_create(const de_params *pin, de_problem **out)
+{
+    if (!pin || !out) return set_error(DE_E_INVALID, "null argument");
+    *out = nullptr;
+    de_params p = *pin;
+    if (p.nelec != 1 && p.nelec != 2) return set_error(DE_E_INVALID, "nelec must be 1 or 2 (got %d)", p.nelec);
+    if (p.n < 1) return set_error(DE_E_INVALID, "N must be >= 1 (got %d)", p.n);
+    const int nn = 2 * p.n + 1;
+    if (nn > 23)
+        return set_error(DE_E_UNSUPPORTED, "N=%d: grids above NN=23 are not built in this version", p.n);
+    if (p.nsmall < 1 || p.tfactor < 1) return set_error(DE_E_INVALID, "nsmall/tfactor must be positive");
+    double delta = p.autodelta ? p.radius / p.n : p.delta;  // INIT_STRUCTS input.F90:384
+    if (!(delta > 0.0)) return set_error(DE_E_INVALID, "grid spacing must be positive");
+    const int nbig_alloc = nn;  // PARAMS%NBIG = 2N+1 (initmod.F90:39)
+    const int nbig_solve = p.nsmall * p.tfactor;
+    if (nbig_solve < nbig_alloc) return set_error(DE_E_INVALID, "nbig lt nout (%d < %d)", nbig_solve, nbig_alloc);
+
+    cudaError_t ce = cudaSetDevice(p.device);
+    if (ce != cudaSuccess) return cuda_error(ce, "cudaSetDevice");
+
+    std::unique_ptr<de_problem> h(new de_problem());
+    h->p = p;
+    h->n = p.n;
+    h->nn = nn;
+    h->m = (int64_t)nn * nn * nn;
+    h->dim = (p.nelec == 2) ? h->m * h->m : h->m;
+    h->delta = delta;
+    DE_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
+
+    // T = KEMATRIX / SCALE^2; V scaled by 1/SCALE (initmod.F90:48,208,224)
+    const cplx scale(std::cos(p.theta), std::sin(p.theta));
+    const cplx s2 = 1.0 / (scale * scale), vs = 1.0 / scale;
+    HamDev &hd = h->ham;
+    hd.nn = nn;
+    hd.nelec = p.nelec;
+    hd.m = h->m;
+    std::vector<double> t = kematrix(nn, delta);
+    for (int d = 0; d < nn; ++d) hd.t[d] = t[d];  // T(d,0) = T(0,d)
+    hd.s2re = s2.real();
+    hd.s2im = s2.imag();
+    hd.vsre = vs.real();
+    hd.vsim = vs.imag();
+
+    auto tinv = cached_tinv(nbig_alloc, nbig_solve, p.nsmall, delta);
+    const int nbd = 2 * nbig_alloc + 1;
+    double *d_tinv = nullptr;
+    DE_CUDA(cudaMalloc(&d_tinv, tinv->size() * sizeof(double)));
+    const int64_t w = 2 * nn - 1;
+    DE_CUDA(cudaMalloc(&h->d_t1a, h->m * sizeof(double)));
+    DE_CUDA(cudaMalloc(&h->d_v12, w * w * w * sizeof(double)));
+    DE_CUDA(cudaMemcpyAsync(d_tinv, tinv->data(), tinv->size() * sizeof(double), cudaMemcpyHostToDevice,
+                            h->stream));
+    ce = build_tables_launch(nn, p.n, p.charge, delta, d_tinv, nbd, h->d_t1a, h->d_v12, h->stream);
+    if (ce != cudaSuccess) return cuda_error(ce, "build_tables");
+    DE_CUDA(cudaStreamSynchronize(h->stream));
+    cudaFree(d_tinv);
+    hd.t1a = h->d_t1a;
+    hd.v12 = h->d_v12;
+
+    DE_CUDA(cudaMalloc(&h->d_small, 64 * 256 * sizeof(double2)));
+    DE_CUDA(cudaMallocHost(&h->h_small, 64 * 256 * sizeof(double2)));
+    *out = h.release();
+    return DE_OK;
+}
+
+DE_API int de_problem_destroy(de_problem *h)
+{
+    if (!h) return DE_OK;
+    cudaSetDevice(h->p.device);
+    if (h->own_stream) cudaStreamSynchronize(h->own_stream);
+    cudaFree(h->d_t1a);
+    cudaFree(h->d_v12);
+    cudaFree(h->d_x);
+    cudaFree(h->d_y);
+    cudaFree(h->d_small);
+    cudaFree(h->d_work);
+    cudaFreeHost(h->h_small);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+    return DE_OK;
+}
+
+DE_API int de_problem_dims(const de_problem *h, int *nn, int64_t *m, int64_t *dim)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    if (nn) *nn = h->nn;
+    if (m) *m = h->m;
+    if (dim) *dim = h->dim;
+    return DE_OK;
+}
+
+DE_API int de_set_stream(de_problem *h, void *s)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    h->stream = s ? (cudaStream_t)s : cudaStreamLegacy;
+    return DE_OK;
+}
+
+DE_API int de_hammult_d(de_problem *h, const de_complex *x, de_complex *y, int64_t mm)
+{
+    if (!h || !x || !y) return set_error(DE_E_INVALID, "null argument");
+    if (mm != h->dim) return set_error(DE_E_SIZE, "SIZE ERRORRRR 66: %lld != %lld", (long long)mm, (long long)h->dim);
+    if ((const void *)x == (const void *)y) return set_error(DE_E_INVALID, "x and y must not alias");
+    cudaSetDevice(h->p.device);
+    return h->matblock((const double2 *)x, (double2 *)y, 1);
+}
+
+DE_API int de_matblock_d(de_problem *h, const de_complex *x, de_complex *ax, int64_t m, int64_t mb, int nev)
+{
+    if (!h || !x || !ax) return set_error(DE_E_INVALID, "null argument");
+    if (nev < 1) return set_error(DE_E_INVALID, "nev must be >= 1");
+    if (m * mb != h->dim) return set_error(DE_E_SIZE, "SIZE ERRORRRR 66: %lld != %lld", (long long)(m * mb), (long long)h->dim);
+    if ((const void *)x == (const void *)ax) return set_error(DE_E_INVALID, "x and ax must not alias");
+    cudaSetDevice(h->p.device);
+    return h->matblock((const double2 *)x, (double2 *)ax, nev);
+}
+
+DE_API int de_matblock(de_problem *h, const de_complex *x, de_complex *ax, int64_t m, int64_t mb, int nev)
+{
+    if (!h || !x || !ax) return set_error(DE_E_INVALID, "null argument");
+    if (nev < 1) return set_error(DE_E_INVALID, "nev must be >= 1");
+    if (m * mb != h->dim) return set_error(DE_E_SIZE, "SIZE ERRORRRR 66: %lld != %lld", (long long)(m * mb), (long long)h->dim);
+    std::lock_guard<std::mutex> lk(h->mu);
+    cudaSetDevice(h->p.device);
+    const int64_t n = h->dim * nev;
+    DE_TRY(h->ensure_stage(n));
+    DE_CUDA(cudaMemcpyAsync(h->d_x, x, n * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    DE_TRY(h->matblock(h->d_x, h->d_y, nev));
+    DE_CUDA(cudaMemcpyAsync(ax, h->d_y, n * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    DE_CUDA(cudaStreamSynchronize(h->stream));
+    return DE_OK;
+}
+
+DE_API int de_hammult(de_problem *h, const de_complex *x, de_complex *y, int64_t mm)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    if (mm != h->dim) return set_error(DE_E_SIZE, "SIZE ERRORRRR 66: %lld != %lld", (long long)mm, (long long)h->dim);
+    return de_matblock(h, x, y, h->dim, 1, 1);
+}
+
+DE_API int de_dots_d(de_problem *h, const de_complex *bras, const de_complex *kets, int64_t size, int nbra,
+                     int nket, de_complex *out, int hermitian)
+{
+    if (!h || !bras || !kets || !out) return set_error(DE_E_INVALID, "null argument");
+    if (size < 1 || nbra < 1 || nket < 1) return set_error(DE_E_INVALID, "empty dot");
+    cudaSetDevice(h->p.device);
+    for (int j0 = 0; j0 < nket; j0 += 128)
+        for (int i0 = 0; i0 < nbra; i0 += 64) {
+            ColList L{}, R{};
+            L.n = std::min(64, nbra - i0);
+            R.n = std::min(128, nket - j0);
+            for (int i = 0; i < L.n; ++i) L.a[i] = (const double2 *)bras + (int64_t)(i0 + i) * size;
+            for (int j = 0; j < R.n; ++j) R.a[j] = (const double2 *)kets + (int64_t)(j0 + j) * size;
+            DE_TRY(h->ensure_work(gram_work_elems(L.n, R.n, size)));
+            cudaError_t e = gram_launch(L, R, size, hermitian ? 1 : 0, h->d_small, L.n, h->d_work, h->stream);
+            if (e != cudaSuccess) return cuda_error(e, "gram");
+            DE_CUDA(cudaMemcpyAsync(h->h_small, h->d_small, (size_t)L.n * R.n * sizeof(double2),
+                                    cudaMemcpyDeviceToHost, h->stream));
+            DE_CUDA(cudaStreamSynchronize(h->stream));
+            for (int j = 0; j < R.n; ++j)
+                for (int i = 0; i < L.n; ++i) {
+                    const double2 v = h->h_small[i + L.n * j];
+                    out[(i0 + i) + (int64_t)nbra * (j0 + j)] = de_complex{v.x, v.y};
+                }
+        }
+    return DE_OK;
+}
+
+DE_API int de_dots(de_problem *h, const de_complex *bras, const de_complex *kets, int64_t size, int nbra,
+                   int nket, de_complex *out, int hermitian)
+{
+    if (!h || !bras || !kets || !out) return set_error(DE_E_INVALID, "null argument");
+    if (size < 1 || nbra < 1 || nket < 1) return set_error(DE_E_INVALID, "empty dot");
+    std::lock_guard<std::mutex> lk(h->mu);
+    cudaSetDevice(h->p.device);
+    double2 *db = nullptr, *dk = nullptr;
+    DE_CUDA(cudaMalloc(&db, (size_t)size * nbra * sizeof(double2)));
+    cudaError_t e = cudaMalloc(&dk, (size_t)size * nket * sizeof(double2));
+    if (e != cudaSuccess) {
+        cudaFree(db);
+        return cuda_error(e, "cudaMalloc");
+    }
+    int s = DE_OK;
+    if ((e = cudaMemcpyAsync(db, bras, (size_t)size * nbra * sizeof(double2), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(dk, kets, (size_t)size * nket * sizeof(double2), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
+        s = cuda_error(e, "cudaMemcpyAsync");
+    if (s == DE_OK) s = de_dots_d(h, (const de_complex *)db, (const de_complex *)dk, size, nbra, nket, out, hermitian);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(db);
+    cudaFree(dk);
+    return s;
+}
+
+DE_API int de_get_expects(de_problem *h, const de_complex *psi, int nvec, int cshiftopt, de_complex *expects)
+{
+    if (!h || !psi || !expects || nvec < 1) return set_error(DE_E_INVALID, "bad argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    cudaSetDevice(h->p.device);
+    DE_TRY(h->ensure_stage(h->dim));
+    DE_TRY(h->ensure_work(dotdiag_work_elems(2, h->dim)));
+    for (int j = 0; j < nvec; ++j) {
+        DE_CUDA(cudaMemcpyAsync(h->d_x, psi + (int64_t)j * h->dim, h->dim * sizeof(double2),
+                                cudaMemcpyHostToDevice, h->stream));
+        DE_TRY(h->matblock(h->d_x, h->d_y, 1));
+        const double2 *a[2] = {h->d_x, h->d_x}, *b[2] = {h->d_y, h->d_x};
+        cudaError_t e = dotdiag_launch(a, b, 2, h->dim, cshiftopt ? 0 : 1, h->d_small, h->d_work, h->stream);
+        if (e != cudaSuccess) return cuda_error(e, "dotdiag");
+        DE_CUDA(cudaMemcpyAsync(h->h_small, h->d_small, 2 * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+        DE_CUDA(cudaStreamSynchronize(h->stream));
+        const cplx num(h->h_small[0].x, h->h_small[0].y), den(h->h_small[1].x, h->h_small[1].y);
+        const cplx q = num / den;
+        expects[j] = de_complex{q.real(), q.imag()};
+    }
+    return DE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+// de_internal.h -- host-side internals shared by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <complex>
+#include <cstdarg>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/doublyexcited.h"
+#include "de_kernels.h"
+
+namespace de {
+
+using cplx = std::complex<double>;
+
+// ---- errors -----------------------------------------------------------
+int set_error(int code, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what);
+
+#define DE_CUDA(call)                                          \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return ::de::cuda_error(_e, #call); \
+    } while (0)
+#define DE_TRY(call)               \
+    do {                           \
+        int _s = (call);           \
+        if (_s != DE_OK) return _s; \
+    } while (0)
+
+// ---- dense host LAPACK (loaded at run time) ----------------------------
+struct Lapack {
+    bool ok = false;
+    std::string path;
+    void (*zggev)(const char *, const char *, const int *, cplx *, const int *, cplx *, const int *,
+                  cplx *, cplx *, cplx *, const int *, cplx *, const int *, cplx *, const int *,
+                  double *, int *, size_t, size_t) = nullptr;
+    void (*zpotrf)(const char *, const int *, cplx *, const int *, int *, size_t) = nullptr;
+    void (*zgesdd)(const char *, const int *, const int *, cplx *, const int *, double *, cplx *,
+                   const int *, cplx *, const int *, cplx *, const int *, double *, int *, int *,
+                   size_t) = nullptr;
+};
+const Lapack &lapack();  // loads once; check .ok
+
+// ---- operator set-up (host) --------------------------------------------
+// GETINVERSE tooth.f90:14-101 on (-nout..nout)^3 (column-major).
+std::vector<double> getinverse(int nout, int nbig, int nsmall, double delta);
+// KEMATRIX hammod.F90:235-260 (real), column-major nn x nn.
+std::vector<double> kematrix(int nn, double delta);
+// Symmetric eigen-decomposition (cyclic Jacobi): a = V diag(e) V^T.
+void jacobi_eigen(int n, std::vector<double> a, std::vector<double> &e, std::vector<double> &v);
+
+// ---- small dense helpers (host) -----------------------------------------
+// Upper Cholesky R of a Hermitian k x k (column-major); returns LAPACK info.
+int zpotrf_upper(int k, std::vector<cplx> &a);
+// Inverse of an upper-triangular k x k matrix (column-major).
+std::vector<cplx> upper_inverse(int k, const std::vector<cplx> &r);
+// gen_cmatsub flag=2 (hr_eigen.f90:223-291): returns DE status.
+int herm_sqrt_pair(int k, const std::vector<cplx> &g, std::vector<cplx> &ginvsqrt,
+                   std::vector<cplx> &gsqrt);
+// SOLVE_GEVP gplmr.F90:395-439 (zggev, |alpha/beta| ascending): vr is
+// kdim x nev column-major.
+int solve_gevp(int kdim, int nev, std::vector<cplx> kp, std::vector<cplx> mp,
+               std::vector<cplx> &vr, std::vector<cplx> *eigs = nullptr);
+
+}  // namespace de
+
+// ---- the handle -----------------------------------------------------------
+struct de_problem {
+    de_params p{};
+    int n = 0, nn = 0;
+    int64_t m = 0, dim = 0;
+    double delta = 0.0;
+    de::HamDev ham{};
+    double *d_t1a = nullptr, *d_v12 = nullptr;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    // staging buffers for host-pointer calls
+    double2 *d_x = nullptr, *d_y = nullptr;
+    int64_t stage_elems = 0;
+    // small scratch
+    double2 *d_small = nullptr;   // 64 x 256 complex
+    double2 *d_work = nullptr;    // reduction partials
+    int64_t work_elems = 0;
+    double2 *h_small = nullptr;   // pinned mirror of d_small
+    std::mutex mu;
+
+    int ensure_stage(int64_t elems);
+    int ensure_work(int64_t elems);
+    int matblock(const double2 *x, double2 *y, int nvec);  // device pointers
+};

@@ -1,0 +1,85 @@
+// de_kernels.h -- launch interface of the sm_100a kernels (host side).
+//
+// Device vectors are double2 arrays (re, im) in the reference layout
+// X(p,q), p = i + NN*j + NN^2*k fastest (hammod.F90:149).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace de {
+
+constexpr int kMaxNN = 27;      // N <= 13 (the reference ran N = 5..15)
+constexpr int kMaxCols = 128;   // columns per block-op operand list
+
+// Operator data for one problem (HAMILTONIAN, structs.F90:87-102).
+struct HamDev {
+    int nn;                 // NN = 2N+1
+    int nelec;              // 1 or 2
+    int64_t m;              // NN^3
+    double t[kMaxNN];       // T_real(0,d) = KEMATRIX first column, d = 0..NN-1
+    double s2re, s2im;      // 1/SCALE^2 (initmod.F90:208)
+    double vsre, vsim;      // 1/SCALE (initmod.F90:224)
+    const double *t1a;      // [M]  A*TINV(r_p), A = -Z/delta^3 (hammod.F90:576-577)
+    const double *v12;      // [(2NN-1)^3] TINV(r_q - r_p)/delta^3 (hammod.F90:578)
+};
+
+// Y(:,:,v) = H X(:,:,v) for v < nvec; vectors are vstride elements apart.
+// Two passes: electron-2 axes + potential (strided cubes, writes Y), then
+// electron-1 axes (contiguous cubes, Y += ...).  Deterministic (no atomics).
+cudaError_t hammult_launch(const HamDev &h, const double2 *x, double2 *y, int nvec,
+                           int64_t vstride, cudaStream_t st);
+
+// One-electron H (NELEC=1): KEMULT1 + V (hammod.F90:71-134).
+cudaError_t hammult1_launch(const HamDev &h, const double *vfull, const double2 *x, double2 *y,
+                            int nvec, int64_t vstride, cudaStream_t st);
+
+// Column list: column c is a[c] - sigma * b[c] (b[c] may be null).
+struct ColList {
+    const double2 *a[kMaxCols];
+    const double2 *b[kMaxCols];
+    double2 sigma;
+    int n;
+};
+
+// G(i,j) = sum_r op(L_i[r]) R_j[r] over len rows; op = conj (herm=1) or
+// identity (herm=0).  out is device memory, column-major with leading
+// dimension ldo; nl <= 64, nr <= 128.  work must hold gram_work_elems().
+int64_t gram_work_elems(int nl, int nr, int64_t len);
+cudaError_t gram_launch(const ColList &L, const ColList &R, int64_t len, int herm, double2 *out,
+                        int ldo, double2 *work, cudaStream_t st);
+
+// Y_j = beta_j * Y_j + alpha * sum_i X_i C(i,j) for j < nout (nout <= 16,
+// nin <= kMaxCols); C is DEVICE memory (complex, column-major, ldc).  Each
+// row is read before it is written, so Y may alias X columns.
+struct UpdList {
+    const double2 *x[kMaxCols];
+    double2 *y[16];
+    double2 beta[16];
+    double2 alpha;  // Y_j = beta_j Y_j + alpha * sum_i X_i C(i,j)
+    int nin, nout;
+};
+cudaError_t update_launch(const UpdList &U, const double2 *c_dev, int ldc, int64_t len,
+                          cudaStream_t st);
+
+// out_j = a_j + s * c_j * b_j, c_j from DEVICE memory (j < n, n <= 64).
+// c_dev may be null (c_j = 1).  out may alias a.
+cudaError_t axpc_launch(double2 *const *out, const double2 *const *a, const double2 *const *b,
+                        int n, double2 s, const double2 *c_dev, int64_t len, cudaStream_t st);
+
+// d_j = sum_r conj(A_j[r]) B_j[r] (herm) for j < n (n <= 64) into DEVICE out.
+int64_t dotdiag_work_elems(int n, int64_t len);
+cudaError_t dotdiag_launch(const double2 *const *a, const double2 *const *b, int n, int64_t len,
+                           int herm, double2 *out, double2 *work, cudaStream_t st);
+
+// x_j *= c_j (c from DEVICE, complex), in place.
+cudaError_t scale_cols_launch(double2 *const *x, int n, const double2 *c_dev, int64_t len,
+                              cudaStream_t st);
+
+// c_j = 1/sqrt(|d_j|) on device (myhgramschmidt_many normalisation).
+cudaError_t inv_sqrt_abs_launch(const double2 *d, double2 *c, int n, cudaStream_t st);
+
+// Potential-table construction on device from the TINV table.
+cudaError_t build_tables_launch(int nn, int n, double charge, double delta, const double *tinv,
+                                int nbd, double *t1a, double *v12, cudaStream_t st);
+
+}  // namespace de

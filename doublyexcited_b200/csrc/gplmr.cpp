@@ -1,0 +1,626 @@
+// gplmr.cpp -- the GPLMR block eigensolver and its BASIC inner solve,
+// device resident: every D-length vector stays in HBM; only k x k matrices
+// (k <= 64) cross to the host for zpotrf / zgesdd / zggev.
+//
+// Reference: GPLMR_EIG gplmr.F90:9-374, SOLVE_GEVP :395-439, MATBLOCK
+// :443-462, PRECBLOCK :466-502, PRECBLOCK_BASIC :674-770; lamod.f90:21-180;
+// basicblocklansolve / harm_orthog_oneblock / fast_harmritz_setup /
+// myhgramschmidt_many harmonic_ritz_small.F90:28-324; gen_cmatsub
+// hr_eigen.f90:223-291.
+//
+// Differences from the reference that do not change results:
+//  * K = (A-sigma)^H (A-sigma) and M = (A-sigma)^H V are formed in ONE Gram
+//    launch over the column lists, with the shift applied as the columns are
+//    loaded (the reference materialises ASIGMAX/W/S/P, gplmr.F90:201-203,244).
+//  * In fast_harmritz_setup the first Krylov block's (H - sigma) V_1 is the
+//    product the orthonormality self-check of harm_orthog_oneblock has just
+//    computed for the same vectors; it is reused (the matvec is
+//    deterministic, so the bits are identical).  stats.matvecs counts the
+//    products executed, stats.matvecs_reference the reference's count.
+//  * lansimpleham / lansimpleovl / lansimplemultovl of fast_harmritz_setup
+//    (harmonic_ritz_small.F90:145-156) never reach the solution and are not
+//    formed; only the first block column of lanham is (rhs is zero below it,
+//    :309-316).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "de_internal.h"
+
+using namespace de;
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+static double secs(clk::time_point a, clk::time_point b)
+{
+    return std::chrono::duration<double>(b - a).count();
+}
+
+struct Solver {
+    de_problem *h;
+    cudaStream_t st;
+    int64_t D;
+    int nev, ns, ldr, nproj, order;
+    cplx sigma;
+    de_gmres gm;
+    bool compat;
+
+    // device blocks (each D x k, column-major)
+    double2 *X = nullptr, *AX = nullptr, *W = nullptr, *AW = nullptr;
+    double2 *S = nullptr, *AS = nullptr, *P = nullptr, *AP = nullptr;
+    double2 *LV = nullptr, *LQ = nullptr;  // inner solve: order*nev each
+    double2 *dG = nullptr, *dC = nullptr, *dE = nullptr, *dR = nullptr, *dT = nullptr;
+    double2 *hbuf = nullptr;  // pinned 64 x 128
+    std::vector<double2 *> allocs;
+
+    int64_t mv_exec = 0, mv_ref = 0;
+    double t_mv = 0, t_prec = 0, t_dense = 0;
+
+    ~Solver()
+    {
+        for (auto p : allocs) cudaFree(p);
+        if (hbuf) cudaFreeHost(hbuf);
+    }
+
+    double2 *col(double2 *b, int j) const { return b + (int64_t)j * D; }
+
+    int alloc(double2 **p, int64_t elems)
+    {
+        cudaError_t e = cudaMalloc(p, elems * sizeof(double2));
+        if (e != cudaSuccess) return cuda_error(e, "cudaMalloc (GPLMR workspace)");
+        allocs.push_back(*p);
+        return DE_OK;
+    }
+
+    int setup()
+    {
+        DE_TRY(alloc(&AX, D * nev));
+        DE_TRY(alloc(&W, D * nev));
+        DE_TRY(alloc(&AW, D * nev));
+        DE_TRY(alloc(&P, D * nev));
+        DE_TRY(alloc(&AP, D * nev));
+        if (ldr > 0) {
+            DE_TRY(alloc(&S, D * ldr));
+            DE_TRY(alloc(&AS, D * ldr));
+        }
+        if (order > 0) {
+            DE_TRY(alloc(&LV, D * (int64_t)std::max(1, order) * nev));
+            DE_TRY(alloc(&LQ, D * (int64_t)std::max(1, order) * nev));
+        }
+        DE_TRY(alloc(&dG, 64 * 128));
+        DE_TRY(alloc(&dC, 128 * 16));
+        DE_TRY(alloc(&dE, 64));
+        DE_TRY(alloc(&dR, 64));
+        DE_TRY(alloc(&dT, 64));
+        DE_CUDA(cudaMallocHost(&hbuf, 64 * 128 * sizeof(double2)));
+        const int64_t wk = std::max<int64_t>(gram_work_elems(64, 128, D), dotdiag_work_elems(64, D));
+        DE_TRY(h->ensure_work(wk));
+        return DE_OK;
+    }
+
+    // ---- primitives ----------------------------------------------------
+    int matblock(const double2 *x, double2 *y, int k)
+    {
+        auto t0 = clk::now();
+        mv_exec += k;
+        mv_ref += k;
+        int s = h->matblock(x, y, k);
+        t_mv += secs(t0, clk::now());
+        return s;
+    }
+
+    // The inner solve's multiplication callback (allhmultsub gplmr.F90:704-716).
+    int inner_mult(const double2 *x, double2 *y, int k)
+    {
+        if (!compat) {
+            mv_exec += k;
+            mv_ref += k;
+            return h->matblock(x, y, k);
+        }
+        mv_exec += 1;
+        mv_ref += 1;
+        DE_TRY(h->matblock(x, y, 1));
+        if (k > 1) DE_CUDA(cudaMemsetAsync(y + D, 0, (size_t)(k - 1) * D * sizeof(double2), st));
+        return DE_OK;
+    }
+
+    static ColList cols(double2 *base, int k, int64_t D, double2 *sub = nullptr, cplx sg = 0.0)
+    {
+        ColList L{};
+        L.n = k;
+        L.sigma = make_double2(sg.real(), sg.imag());
+        for (int j = 0; j < k; ++j) {
+            L.a[j] = base + (int64_t)j * D;
+            L.b[j] = sub ? sub + (int64_t)j * D : nullptr;
+        }
+        return L;
+    }
+
+    int gram_dev(const ColList &L, const ColList &R, double2 *out, int ldo, int herm = 1)
+    {
+        cudaError_t e = gram_launch(L, R, D, herm, out, ldo, h->d_work, st);
+        if (e != cudaSuccess) return cuda_error(e, "gram");
+        return DE_OK;
+    }
+
+    int gram_host(const ColList &L, const ColList &R, std::vector<cplx> &g)
+    {
+        DE_TRY(gram_dev(L, R, dG, L.n));
+        DE_CUDA(cudaMemcpyAsync(hbuf, dG, (size_t)L.n * R.n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        DE_CUDA(cudaStreamSynchronize(st));
+        g.resize((size_t)L.n * R.n);
+        for (size_t i = 0; i < g.size(); ++i) g[i] = cplx(hbuf[i].x, hbuf[i].y);
+        return DE_OK;
+    }
+
+    int upload(const std::vector<cplx> &m, double2 *dst)
+    {
+        for (size_t i = 0; i < m.size(); ++i) hbuf[i] = make_double2(m[i].real(), m[i].imag());
+        DE_CUDA(cudaMemcpyAsync(dst, hbuf, m.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+        DE_CUDA(cudaStreamSynchronize(st));  // hbuf is reused
+        return DE_OK;
+    }
+
+    // Y = beta Y + alpha sum_i Xsrc_i C(i, j);  xs / ys are column pointers.
+    int update(const std::vector<const double2 *> &xs, const std::vector<double2 *> &ys,
+               const double2 *c, int ldc, cplx alpha, cplx beta)
+    {
+        UpdList U{};
+        U.nin = (int)xs.size();
+        U.nout = (int)ys.size();
+        if (U.nin > kMaxCols || U.nout > 16) return set_error(DE_E_INVALID, "update too wide");
+        for (int i = 0; i < U.nin; ++i) U.x[i] = xs[i];
+        for (int j = 0; j < U.nout; ++j) {
+            U.y[j] = ys[j];
+            U.beta[j] = make_double2(beta.real(), beta.imag());
+        }
+        U.alpha = make_double2(alpha.real(), alpha.imag());
+        cudaError_t e = update_launch(U, c, ldc, D, st);
+        if (e != cudaSuccess) return cuda_error(e, "update");
+        return DE_OK;
+    }
+
+    std::vector<const double2 *> cl(const double2 *b, int k) const
+    {
+        std::vector<const double2 *> v(k);
+        for (int j = 0; j < k; ++j) v[j] = b + (int64_t)j * D;
+        return v;
+    }
+    std::vector<double2 *> clw(double2 *b, int k) const
+    {
+        std::vector<double2 *> v(k);
+        for (int j = 0; j < k; ++j) v[j] = b + (int64_t)j * D;
+        return v;
+    }
+
+    // B <- B - Q (Q^H B): crossmult + ZGEMM('N','N',...,-1,...,1)
+    int orth_against(double2 *q, int kq, double2 *b, int kb, double2 *aq = nullptr, double2 *ab = nullptr)
+    {
+        DE_TRY(gram_dev(cols(q, kq, D), cols(b, kb, D), dG, kq));
+        DE_TRY(update(cl(q, kq), clw(b, kb), dG, kq, -1.0, 1.0));
+        if (aq) DE_TRY(update(cl(aq, kq), clw(ab, kb), dG, kq, -1.0, 1.0));
+        return DE_OK;
+    }
+
+    // cholQR lamod.f90:128-180; returns R (k x k upper) and applies X <- X R^{-1}.
+    int cholqr(double2 *x, int k, std::vector<cplx> &r)
+    {
+        DE_TRY(gram_host(cols(x, k, D), cols(x, k, D), r));
+        auto t0 = clk::now();
+        double rsum = 0.0;
+        for (auto &v : r) rsum += std::abs(v);
+        if (rsum == 0.0) return set_error(DE_E_CHOLESKY, "cholQR of an all-zero block (rsum=0)");
+        const int info = zpotrf_upper(k, r);
+        if (info == -1000) return set_error(DE_E_LAPACK, "host LAPACK not found (set DE_LAPACK_LIB)");
+        if (info != 0) return set_error(DE_E_CHOLESKY, "Cholesky failed!!! info=%d", info);
+        t_dense += secs(t0, clk::now());
+        return trsm(x, k, r);
+    }
+
+    // X <- X R^{-1} (ZTRSM 'R','U','N','N')
+    int trsm(double2 *x, int k, const std::vector<cplx> &r)
+    {
+        DE_TRY(upload(upper_inverse(k, r), dC));
+        return update(cl(x, k), clw(x, k), dC, k, 1.0, 0.0);
+    }
+
+    // x_j <- x_j / ||x_j|| for two blocks sharing the factor (lamod normalize)
+    int normalize(double2 *x, int k, double2 *ax = nullptr)
+    {
+        std::vector<const double2 *> a = cl(x, k);
+        cudaError_t e = dotdiag_launch(a.data(), a.data(), k, D, 1, dR, h->d_work, st);
+        if (e != cudaSuccess) return cuda_error(e, "dotdiag");
+        if ((e = inv_sqrt_abs_launch(dR, dT, k, st)) != cudaSuccess) return cuda_error(e, "inv_sqrt");
+        std::vector<double2 *> w = clw(x, k);
+        if ((e = scale_cols_launch(w.data(), k, dT, D, st)) != cudaSuccess) return cuda_error(e, "scale");
+        if (ax) {
+            w = clw(ax, k);
+            if ((e = scale_cols_launch(w.data(), k, dT, D, st)) != cudaSuccess) return cuda_error(e, "scale");
+        }
+        return DE_OK;
+    }
+
+    // out_j = a_j - E_j b_j with E on device (dE)
+    int minus_e(double2 *out, const double2 *a, const double2 *b, int k)
+    {
+        std::vector<double2 *> o = clw(out, k);
+        std::vector<const double2 *> aa = cl(a, k), bb = cl(b, k);
+        cudaError_t e = axpc_launch(o.data(), aa.data(), bb.data(), k, make_double2(-1.0, 0.0), dE, D, st);
+        if (e != cudaSuccess) return cuda_error(e, "axpc");
+        return DE_OK;
+    }
+
+    // E = diag(X^H AX); W = AX - X E; resnrm = sqrt(diag(W^H W)) -> host
+    int residuals(std::vector<cplx> &e_host, std::vector<double> &res)
+    {
+        std::vector<const double2 *> xx = cl(X, nev), aa = cl(AX, nev), ww = cl(W, nev);
+        cudaError_t e = dotdiag_launch(xx.data(), aa.data(), nev, D, 1, dE, h->d_work, st);
+        if (e != cudaSuccess) return cuda_error(e, "dotdiag");
+        DE_TRY(minus_e(W, AX, X, nev));
+        if ((e = dotdiag_launch(ww.data(), ww.data(), nev, D, 1, dR, h->d_work, st)) != cudaSuccess)
+            return cuda_error(e, "dotdiag");
+        DE_CUDA(cudaMemcpyAsync(hbuf, dE, nev * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        DE_CUDA(cudaMemcpyAsync(hbuf + 64, dR, nev * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        DE_CUDA(cudaStreamSynchronize(st));
+        e_host.resize(nev);
+        res.resize(nev);
+        for (int j = 0; j < nev; ++j) {
+            e_host[j] = cplx(hbuf[j].x, hbuf[j].y);
+            res[j] = std::sqrt(hbuf[64 + j].x);
+            if (!std::isfinite(res[j]) || !std::isfinite(e_host[j].real()) || !std::isfinite(e_host[j].imag()))
+                return set_error(DE_E_NAN, "non-finite residual or eigenvalue in column %d", j);
+        }
+        return DE_OK;
+    }
+
+    // ---- inner solve -------------------------------------------------------
+    // myhgramschmidt_many with factors (1,0): two classical passes of the
+    // (H-sigma)-weighted Gram-Schmidt of the pair (q, v) against the first m
+    // pairs of (LQ, LV).
+    int hgram(int m, double2 *q, double2 *v)
+    {
+        for (int pass = 0; pass < 2; ++pass) {
+            if (m > 0) {
+                DE_TRY(gram_dev(cols(LQ, m, D), cols(q, 1, D), dT, m));
+                DE_TRY(update(cl(LQ, m), {q}, dT, m, -1.0, 1.0));
+                DE_TRY(update(cl(LV, m), {v}, dT, m, -1.0, 1.0));
+            }
+            const double2 *qa[1] = {q};
+            cudaError_t e = dotdiag_launch(qa, qa, 1, D, 1, dR, h->d_work, st);
+            if (e != cudaSuccess) return cuda_error(e, "dotdiag");
+            if ((e = inv_sqrt_abs_launch(dR, dR + 1, 1, st)) != cudaSuccess) return cuda_error(e, "inv_sqrt");
+            double2 *qv[2] = {q, v};
+            if ((e = scale_cols_launch(qv, 1, dR + 1, D, st)) != cudaSuccess) return cuda_error(e, "scale");
+            if ((e = scale_cols_launch(qv + 1, 1, dR + 1, D, st)) != cudaSuccess) return cuda_error(e, "scale");
+        }
+        return DE_OK;
+    }
+
+    // basicblocklansolve harmonic_ritz_small.F90:258-324 on block b (k
+    // columns), in place: b <- V (Q^H V_1) G^{1/2}.
+    int basic(double2 *b, int k)
+    {
+        const cplx ms = -sigma;
+        const double2 msg = make_double2(ms.real(), ms.imag());
+        // harm_orthog_oneblock :161-244
+        DE_CUDA(cudaMemcpyAsync(LV, b, (size_t)k * D * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+        DE_TRY(inner_mult(LV, LQ, k));
+        {
+            std::vector<double2 *> o = clw(LQ, k);
+            std::vector<const double2 *> a = cl(LQ, k), v = cl(LV, k);
+            cudaError_t e = axpc_launch(o.data(), a.data(), v.data(), k, msg, nullptr, D, st);
+            if (e != cudaSuccess) return cuda_error(e, "axpc");
+        }
+        std::vector<cplx> g, ginv, gsq;
+        DE_TRY(gram_host(cols(LQ, k, D), cols(LQ, k, D), g));
+        auto t0 = clk::now();
+        DE_TRY(herm_sqrt_pair(k, g, ginv, gsq));
+        t_dense += secs(t0, clk::now());
+        std::vector<cplx> ginvh((size_t)k * k);
+        for (int j = 0; j < k; ++j)
+            for (int i = 0; i < k; ++i) ginvh[i + (size_t)k * j] = std::conj(ginv[j + (size_t)k * i]);
+        DE_TRY(upload(ginvh, dC));
+        DE_TRY(update(cl(LV, k), clw(LV, k), dC, k, 1.0, 0.0));
+        // self-check: (H - sigma) V_1 orthonormal to 1e-10
+        DE_TRY(inner_mult(LV, LQ, k));
+        {
+            std::vector<double2 *> o = clw(LQ, k);
+            std::vector<const double2 *> a = cl(LQ, k), v = cl(LV, k);
+            cudaError_t e = axpc_launch(o.data(), a.data(), v.data(), k, msg, nullptr, D, st);
+            if (e != cudaSuccess) return cuda_error(e, "axpc");
+        }
+        std::vector<cplx> chk;
+        DE_TRY(gram_host(cols(LQ, k, D), cols(LQ, k, D), chk));
+        for (int j = 0; j < k; ++j)
+            for (int i = 0; i < k; ++i) {
+                const cplx v = chk[i + (size_t)k * j] - (i == j ? 1.0 : 0.0);
+                if (std::abs(v) > 1e-10) return set_error(DE_E_ORTHO, "AACK DOTS: |T(%d,%d)-I| = %.3e", i, j, std::abs(v));
+            }
+        // fast_harmritz_setup :86-158 (maxiter = M^2 never truncates a block)
+        for (int io = 0; io < order; ++io) {
+            double2 *vb = col(LV, io * k), *qb = col(LQ, io * k);
+            if (io > 0) DE_TRY(inner_mult(col(LV, (io - 1) * k), vb, k));
+            if (io > 0) {
+                DE_TRY(inner_mult(vb, qb, k));
+            } else {
+                mv_ref += compat ? 1 : k;  // the reference recomputes the product checked above
+            }
+            if (io > 0) {
+                std::vector<double2 *> o = clw(qb, k);
+                std::vector<const double2 *> a = cl(qb, k), v = cl(vb, k);
+                cudaError_t e = axpc_launch(o.data(), a.data(), v.data(), k, msg, nullptr, D, st);
+                if (e != cudaSuccess) return cuda_error(e, "axpc");
+            }
+            for (int i = 0; i < k; ++i) DE_TRY(hgram(io * k + i, col(qb, i), col(vb, i)));
+        }
+        // solution: V (lanham rhs), rhs(:,1,:) = G^{1/2} (:309-316)
+        const int thisdim = order * k;
+        std::vector<cplx> g1;  // Q^H V_1, thisdim x k (first block column of lanham)
+        DE_TRY(gram_host(cols(LQ, thisdim, D), cols(LV, k, D), g1));
+        std::vector<cplx> sv((size_t)thisdim * k, 0.0);
+        for (int j = 0; j < k; ++j)
+            for (int i = 0; i < thisdim; ++i) {
+                cplx s = 0.0;
+                for (int l = 0; l < k; ++l) s += g1[i + (size_t)thisdim * l] * gsq[l + (size_t)k * j];
+                sv[i + (size_t)thisdim * j] = s;
+            }
+        DE_TRY(upload(sv, dC));
+        return update(cl(LV, thisdim), clw(b, k), dC, thisdim, 1.0, 0.0);
+    }
+
+    // PRECBLOCK gplmr.F90:466-502 (in place)
+    int precblock(double2 *b, int k)
+    {
+        auto t0 = clk::now();
+        int s;
+        if (order == 1) {
+            s = matblock(b, LQ, k);
+            if (s == DE_OK) {
+                cudaError_t e = cudaMemcpyAsync(b, LQ, (size_t)k * D * sizeof(double2), cudaMemcpyDeviceToDevice, st);
+                if (e != cudaSuccess) s = cuda_error(e, "copy");
+            }
+        } else if (gm.usepetscflag == 0) {
+            s = set_error(DE_E_UNSUPPORTED, "usepetscflag=0 selects the PETSc KSP inner solve, which this build does not provide");
+        } else {
+            s = basic(b, k);
+        }
+        t_prec += secs(t0, clk::now());
+        return s;
+    }
+
+    // ---- main loop -------------------------------------------------------
+    int run(double2 *x_dev, de_complex *e_out, int maxit, double tol, int outmodulus, de_stats *stats)
+    {
+        auto tstart = clk::now();
+        X = x_dev;
+        DE_TRY(setup());
+        DE_TRY(normalize(X, nev));
+        DE_TRY(matblock(X, AX, nev));
+        std::vector<cplx> E;
+        std::vector<double> res;
+        DE_TRY(residuals(E, res));
+        double maxres = *std::max_element(res.begin(), res.end());
+        if (outmodulus > 0) {
+            printf(" GPLMR_EIG STARTED ... \n THE TARGETED SHIFT IS \n (%.15f,%.15f)\n", sigma.real(), sigma.imag());
+            fflush(stdout);
+        }
+        int it = 1;
+        std::vector<cplx> R;
+        while (it <= maxit && maxres > tol) {
+            DE_TRY(cholqr(X, nev, R));
+            DE_TRY(trsm(AX, nev, R));
+            if (gm.max_inner_iter > 0) DE_TRY(precblock(W, nev));
+            DE_TRY(orth_against(X, nev, W, nev));
+            DE_TRY(cholqr(W, nev, R));
+            DE_TRY(matblock(W, AW, nev));
+            if (ns > 0) {
+                DE_TRY(minus_e(S, AW, W, nev));
+                if (gm.max_inner_iter > 0) DE_TRY(precblock(S, nev));
+                DE_TRY(orth_against(X, nev, S, nev));
+                DE_TRY(orth_against(W, nev, S, nev));
+                DE_TRY(cholqr(S, nev, R));
+                DE_TRY(matblock(S, AS, nev));
+                for (int l = 2; l <= ns; ++l) {
+                    const int j1 = (l - 1) * nev;
+                    double2 *sl = col(S, j1), *asl = col(AS, j1);
+                    DE_TRY(minus_e(sl, col(AS, j1 - nev), col(S, j1 - nev), nev));
+                    if (gm.max_inner_iter > 0) DE_TRY(precblock(sl, nev));
+                    DE_TRY(orth_against(X, nev, sl, nev));
+                    DE_TRY(orth_against(W, nev, sl, nev));
+                    DE_TRY(orth_against(S, j1, sl, nev));
+                    DE_TRY(cholqr(sl, nev, R));
+                    DE_TRY(matblock(sl, asl, nev));
+                }
+            }
+            if (it > 1) {
+                DE_TRY(orth_against(X, nev, P, nev, AX, AP));
+                DE_TRY(orth_against(W, nev, P, nev, AW, AP));
+                if (ldr > 0) DE_TRY(orth_against(S, ldr, P, nev, AS, AP));
+                DE_TRY(cholqr(P, nev, R));
+                DE_TRY(trsm(AP, nev, R));
+            }
+            // harmonic projection: K = B^H B, M = B^H V, B = A V - sigma V
+            const int kdim = (it > 1) ? nproj : nproj - nev;
+            ColList B{}, KV{};
+            {
+                struct Pair { double2 *v, *av; int k; };
+                std::vector<Pair> blocks = {{X, AX, nev}, {W, AW, nev}};
+                if (ldr > 0) blocks.push_back({S, AS, ldr});
+                if (it > 1) blocks.push_back({P, AP, nev});
+                int c = 0;
+                B.sigma = make_double2(sigma.real(), sigma.imag());
+                KV.sigma = B.sigma;
+                for (auto &pb : blocks)
+                    for (int j = 0; j < pb.k; ++j, ++c) {
+                        B.a[c] = col(pb.av, j);
+                        B.b[c] = col(pb.v, j);
+                        KV.a[c] = B.a[c];
+                        KV.b[c] = B.b[c];
+                        KV.a[kdim + c] = col(pb.v, j);
+                        KV.b[kdim + c] = nullptr;
+                    }
+                B.n = kdim;
+                KV.n = 2 * kdim;
+            }
+            std::vector<cplx> km;
+            DE_TRY(gram_host(B, KV, km));
+            auto t0 = clk::now();
+            std::vector<cplx> kp(km.begin(), km.begin() + (size_t)kdim * kdim),
+                mp(km.begin() + (size_t)kdim * kdim, km.end()), vr;
+            DE_TRY(solve_gevp(kdim, nev, kp, mp, vr));
+            t_dense += secs(t0, clk::now());
+            // coordinates: rows [0,nev) X, [nev,2nev) W, [2nev,2nev+ldr) S, [2nev+ldr,nproj) P
+            auto rows = [&](int r0, int nr) {
+                std::vector<cplx> m((size_t)nr * nev);
+                for (int j = 0; j < nev; ++j)
+                    for (int i = 0; i < nr; ++i) m[i + (size_t)nr * j] = vr[(r0 + i) + (size_t)kdim * j];
+                return m;
+            };
+            // P <- P CP + S CS + W CW; AP likewise
+            {
+                std::vector<const double2 *> xs, axs;
+                std::vector<cplx> c;
+                auto append = [&](const double2 *v, const double2 *av, int k, const std::vector<cplx> &m) {
+                    for (int j = 0; j < k; ++j) {
+                        xs.push_back(v + (int64_t)j * D);
+                        axs.push_back(av + (int64_t)j * D);
+                    }
+                    (void)m;
+                };
+                std::vector<std::vector<cplx>> parts;
+                if (it > 1) {
+                    append(P, AP, nev, {});
+                    parts.push_back(rows(2 * nev + ldr, nev));
+                }
+                if (ldr > 0) {
+                    append(S, AS, ldr, {});
+                    parts.push_back(rows(2 * nev, ldr));
+                }
+                append(W, AW, nev, {});
+                parts.push_back(rows(nev, nev));
+                const int nin = (int)xs.size();
+                c.assign((size_t)nin * nev, 0.0);
+                int r0 = 0;
+                for (auto &pm : parts) {
+                    const int nr = (int)(pm.size() / nev);
+                    for (int j = 0; j < nev; ++j)
+                        for (int i = 0; i < nr; ++i) c[(r0 + i) + (size_t)nin * j] = pm[i + (size_t)nr * j];
+                    r0 += nr;
+                }
+                DE_TRY(upload(c, dC));
+                DE_TRY(update(xs, clw(P, nev), dC, nin, 1.0, 0.0));
+                DE_TRY(update(axs, clw(AP, nev), dC, nin, 1.0, 0.0));
+            }
+            // X <- X CX + P; AX <- AX CX + AP
+            {
+                std::vector<cplx> cx = rows(0, nev), c((size_t)2 * nev * nev, 0.0);
+                for (int j = 0; j < nev; ++j) {
+                    for (int i = 0; i < nev; ++i) c[i + (size_t)2 * nev * j] = cx[i + (size_t)nev * j];
+                    c[(nev + j) + (size_t)2 * nev * j] = 1.0;
+                }
+                DE_TRY(upload(c, dC));
+                std::vector<const double2 *> xs = cl(X, nev), axs = cl(AX, nev);
+                std::vector<const double2 *> ps = cl(P, nev), aps = cl(AP, nev);
+                xs.insert(xs.end(), ps.begin(), ps.end());
+                axs.insert(axs.end(), aps.begin(), aps.end());
+                DE_TRY(update(xs, clw(X, nev), dC, 2 * nev, 1.0, 0.0));
+                DE_TRY(update(axs, clw(AX, nev), dC, 2 * nev, 1.0, 0.0));
+            }
+            DE_TRY(normalize(X, nev, AX));
+            DE_TRY(residuals(E, res));
+            maxres = *std::max_element(res.begin(), res.end());
+            if (outmodulus > 0 && (maxres <= tol || it % outmodulus == 0)) {
+                printf("ITERATION %5d\n", it);
+                for (int j = 0; j < nev; ++j)
+                    printf("EIG %4d = %20.12f%20.12f,  ERROR = %10.2E\n", j + 1, E[j].real(), E[j].imag(), res[j]);
+                fflush(stdout);
+            }
+            ++it;
+        }
+        DE_CUDA(cudaStreamSynchronize(st));
+        for (int j = 0; j < nev; ++j) e_out[j] = de_complex{E[j].real(), E[j].imag()};
+        if (stats) {
+            stats->iterations = it - 1;
+            stats->converged = maxres <= tol;
+            stats->matvecs = mv_exec;
+            stats->matvecs_reference = mv_ref;
+            stats->max_residual = maxres;
+            stats->t_total_s = secs(tstart, clk::now());
+            stats->t_matvec_s = t_mv;
+            stats->t_prec_s = t_prec;
+            stats->t_dense_s = t_dense;
+        }
+        return DE_OK;
+    }
+};
+
+int check_args(de_problem *h, int64_t m, int64_t mb, int nev, int ns, const de_gmres *gm)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    if (h->p.nelec != 2) return set_error(DE_E_INVALID, "GPLMR_EIG needs the two-electron operator");
+    if (m * mb != h->dim) return set_error(DE_E_SIZE, "SIZE ERRORRRR 66: M*MB=%lld != %lld", (long long)(m * mb), (long long)h->dim);
+    if (nev < 1 || ns < 0) return set_error(DE_E_INVALID, "nev >= 1 and ns >= 0 required");
+    if ((3 + ns) * nev > 64) return set_error(DE_E_INVALID, "(3+NS)*NEV = %d exceeds 64", (3 + ns) * nev);
+    if (nev > 16) return set_error(DE_E_INVALID, "NEV above 16 is not supported");
+    if (gm && gm->max_inner_iter < 0) return set_error(DE_E_INVALID, "max_inner_iter must be >= 0");
+    if (gm && gm->max_inner_iter * nev > 64) return set_error(DE_E_INVALID, "max_inner_iter*NEV exceeds 64");
+    if (!lapack().ok) return set_error(DE_E_LAPACK, "host LAPACK not found (set DE_LAPACK_LIB)");
+    return DE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+DE_API int de_gplmr_eig_d(de_problem *h, de_complex *x_d, de_complex *e, int64_t m, int64_t mb,
+                          de_complex sigma, int nev, int ns, int maxit, double tol, const de_gmres *gm,
+                          int outmodulus, de_stats *stats)
+{
+    DE_TRY(check_args(h, m, mb, nev, ns, gm));
+    if (!x_d || !e) return set_error(DE_E_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    cudaSetDevice(h->p.device);
+    Solver s{};
+    s.h = h;
+    s.st = h->stream;
+    s.D = h->dim;
+    s.nev = nev;
+    s.ns = ns;
+    s.ldr = ns * nev;
+    s.nproj = (3 + ns) * nev;
+    de_gmres g{5, 1, 1e-3, 0};
+    if (gm) g = *gm;
+    s.gm = g;
+    s.order = g.max_inner_iter;
+    s.compat = g.compat_first_column_only != 0;
+    s.sigma = cplx(sigma.re, sigma.im);
+    if (stats) std::memset(stats, 0, sizeof *stats);
+    return s.run((double2 *)x_d, e, maxit, tol, outmodulus, stats);
+}
+
+DE_API int de_gplmr_eig(de_problem *h, de_complex *x, de_complex *e, int64_t m, int64_t mb, de_complex sigma,
+                        int nev, int ns, int maxit, double tol, const de_gmres *gm, int outmodulus, de_stats *stats)
+{
+    DE_TRY(check_args(h, m, mb, nev, ns, gm));
+    if (!x || !e) return set_error(DE_E_INVALID, "null argument");
+    cudaSetDevice(h->p.device);
+    double2 *xd = nullptr;
+    const size_t bytes = (size_t)h->dim * nev * sizeof(double2);
+    DE_CUDA(cudaMalloc(&xd, bytes));
+    int s = DE_OK;
+    cudaError_t ce = cudaMemcpyAsync(xd, x, bytes, cudaMemcpyHostToDevice, h->stream);
+    if (ce != cudaSuccess) s = cuda_error(ce, "H2D");
+    if (s == DE_OK) s = de_gplmr_eig_d(h, (de_complex *)xd, e, m, mb, sigma, nev, ns, maxit, tol, gm, outmodulus, stats);
+    if (s == DE_OK) {
+        ce = cudaMemcpyAsync(x, xd, bytes, cudaMemcpyDeviceToHost, h->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
+        if (ce != cudaSuccess) s = cuda_error(ce, "D2H");
+    }
+    cudaFree(xd);
+    return s;
+}
+
+}  // extern "C"

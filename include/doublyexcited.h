@@ -1,0 +1,227 @@
+/*
+ * doublyexcited.h -- C ABI of the B200 implementation of doublyexcited's
+ * hot path: the complex-scaled two-electron sinc-DVR helium Hamiltonian
+ * applied to blocks of vectors inside the GPLMR harmonic-Ritz block
+ * eigensolver.
+ *
+ * Conventions
+ *   - Every function returns an int status: DE_OK (0) or a DE_E_* code.
+ *     Nothing aborts or exits; de_last_error() gives a message for the
+ *     calling host thread.
+ *   - Complex numbers are de_complex {re, im}: the memory layout of Fortran
+ *     COMPLEX*16 and of C99 double _Complex, so reference-side buffers pass
+ *     through unchanged.
+ *   - Two-electron vectors are X(1:M, 1:M) column-major with electron 1
+ *     (p) fastest, p = i + NN*j + NN^2*k, exactly as the reference stores
+ *     them (hammod.F90:149, gplmr.F90:27).  Blocks are X(M, MB, NEV).
+ *   - One de_problem handle owns all state (operator tables, device
+ *     workspace, CUDA stream).  Calls on one handle are serialised by the
+ *     caller; different handles may be used from different host threads.
+ *     The reference's HAMMULT keeps SAVE'd state and is not reentrant
+ *     (hammod.F90:31,153-159); this API is.
+ *   - Functions without a suffix take HOST pointers and include the
+ *     host<->device copies; the _d variants take DEVICE pointers and run on
+ *     the handle's stream.
+ *
+ * Paths cited below are relative to complexscale-djhnow/code/ of the
+ * reference.
+ */
+#ifndef DOUBLYEXCITED_B200_H
+#define DOUBLYEXCITED_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DE_API __attribute__((visibility("default")))
+
+typedef struct {
+    double re, im;
+} de_complex;
+
+enum {
+    DE_OK = 0,
+    DE_E_INVALID = 1,      /* bad argument */
+    DE_E_SIZE = 2,         /* size mismatch (reference: "SIZE ERRORRRR 66", doublyexcited.F90:33-36) */
+    DE_E_CUDA = 3,         /* CUDA runtime error */
+    DE_E_NOMEM = 4,        /* device or host allocation failed */
+    DE_E_UNSUPPORTED = 5,  /* option the build does not provide (e.g. PETSc inner solve) */
+    DE_E_CHOLESKY = 6,     /* zpotrf breakdown in cholQR (lamod.f90:169-175) */
+    DE_E_GEVP = 7,         /* zggev failure (gplmr.F90:431-432) */
+    DE_E_SVD = 8,          /* zgesdd failure (hr_eigen.f90:246-248) */
+    DE_E_ORTHO = 9,        /* inner-solve orthonormality self-check (harmonic_ritz_small.F90:221-242) */
+    DE_E_NOT_CONVERGED = 10,
+    DE_E_IO = 11,          /* file error */
+    DE_E_PARSE = 12,       /* Input.Inp / argument parse error */
+    DE_E_LAPACK = 13,      /* host LAPACK library not found */
+    DE_E_NAN = 14,         /* non-finite residual */
+    DE_E_BUSY = 15         /* admission refused (serving) */
+};
+
+enum { DE_PREC_FP64 = 0, DE_PREC_MIXED = 1 };
+
+/* Grid / physics parameters.  Mirrors PARAMETERS (structs.F90:28-57) and the
+ * &grid/&molecule/&main namelist fields that feed INIT_STRUCTS
+ * (input.F90:365-417). */
+typedef struct {
+    int n;            /* N: NN = 2N+1 points per axis (input.F90 &grid N) */
+    double delta;     /* grid spacing (DELTA) */
+    double radius;    /* box radius (RADIUS); delta = radius/N when autodelta */
+    int autodelta;    /* AUTODELTA */
+    double theta;     /* complex-scaling angle (THETA); SCALE = exp(i theta) */
+    double charge;    /* nuclear charge (CHARGE), nucleus at the origin */
+    int nelec;        /* 1 or 2 electrons */
+    int nsmall;       /* NSMALL of the TINV solve (default 22) */
+    int tfactor;      /* TFACTOR of the TINV solve (default 4) */
+    int precision;    /* DE_PREC_FP64 or DE_PREC_MIXED */
+    int device;       /* CUDA device ordinal */
+} de_params;
+
+/* Inner-solve options.  Mirrors GMRES_SOLVER (structs.F90:137-162). */
+typedef struct {
+    int max_inner_iter;          /* GM_MAX_INNER_ITER: Krylov order of PRECBLOCK_BASIC */
+    int usepetscflag;            /* 0 -> PETSc KSP path (not built: DE_E_UNSUPPORTED); else BASIC.
+                                    The reference's flag is inverted (gplmr.F90:496-500); same here. */
+    double tol;                  /* GM_TOL (used by the PETSc path only) */
+    int compat_first_column_only;/* 1: reproduce allhmultsub's first-column-only matvec
+                                    (gplmr.F90:704-716); other columns of the product are zero */
+} de_gmres;
+
+/* Solver statistics (the reference prints these, gplmr.F90:343-366). */
+typedef struct {
+    int iterations;
+    int converged;
+    int64_t matvecs;          /* vector-matvecs executed */
+    int64_t matvecs_reference;/* HAMMULT calls the reference makes for the same solve (its ICALLED) */
+    double max_residual;
+    double t_total_s;         /* wall time of the solve */
+    double t_matvec_s;        /* MATBLOCK time (TSPMV) */
+    double t_prec_s;          /* PRECBLOCK time (TPREC) */
+    double t_dense_s;         /* host dense LAPACK time */
+} de_stats;
+
+typedef struct de_problem de_problem;
+
+/* ---- errors ---------------------------------------------------------- */
+DE_API const char *de_strerror(int status);
+DE_API const char *de_last_error(void);
+DE_API const char *de_version(void);
+
+/* ---- parameters and set-up ------------------------------------------- */
+
+/* Reference defaults (input.F90:1-124: N=2, DELTA=0.5, RADIUS=7, AUTODELTA,
+ * THETA=0, CHARGE=2, NSMALL=22, TFACTOR=4) with nelec=2. */
+DE_API void de_params_default(de_params *p);
+
+/* Build the operator: T = KEMATRIX/SCALE^2, TINV by GETINVERSE, potential
+ * tables (INIT_HAMILTONIAN initmod.F90:174-228, GETINVERSE tooth.f90:14-101,
+ * POTENTIAL1/2 hammod.F90:432-582).  Allocates device tables only. */
+DE_API int de_problem_create(const de_params *p, de_problem **out);
+DE_API int de_problem_destroy(de_problem *h);
+
+/* NN, M = NN^3 and the vector length M^nelec of a handle. */
+DE_API int de_problem_dims(const de_problem *h, int *nn, int64_t *m, int64_t *dim);
+
+/* Run the handle's work on a caller's cudaStream_t from now on.  NULL is the
+ * CUDA legacy default stream (as in the CUDA runtime); a new handle uses a
+ * private non-blocking stream until this is called. */
+DE_API int de_set_stream(de_problem *h, void *cuda_stream);
+
+/* ---- operator: HAMMULT / MATBLOCK / MYMATMUL ------------------------- */
+
+/* Y = H X for one vector of length mm (== M^nelec).  Replaces
+ * HAMMULT(HAM,PARAMS,MPIDATA,X,Y,MM) hammod.F90:19-67 at NP=1. */
+DE_API int de_hammult(de_problem *h, const de_complex *x, de_complex *y, int64_t mm);
+DE_API int de_hammult_d(de_problem *h, const de_complex *x_d, de_complex *y_d, int64_t mm);
+
+/* AX(:,:,j) = H X(:,:,j), j = 1..nev, in one launch.  Replaces MATBLOCK
+ * gplmr.F90:443-462 and the MYMATMUL callback doublyexcited.F90:24-44
+ * (m*mb must equal the vector length: DE_E_SIZE otherwise). */
+DE_API int de_matblock(de_problem *h, const de_complex *x, de_complex *ax, int64_t m, int64_t mb,
+                       int nev);
+DE_API int de_matblock_d(de_problem *h, const de_complex *x_d, de_complex *ax_d, int64_t m,
+                         int64_t mb, int nev);
+
+/* OUT(i,j) = <BRA_i, KET_j> over vectors of length size.  hermitian=1:
+ * conj(BRA).KET (MYDOTSUB doublyexcited.F90:47-59, MPIHERMDOT
+ * hammod.F90:383-403); hermitian=0: BRA.KET, the c-product (MPIDOT
+ * hammod.F90:361-380).  out is nbra x nket column-major. */
+DE_API int de_dots(de_problem *h, const de_complex *bras, const de_complex *kets, int64_t size,
+                   int nbra, int nket, de_complex *out, int hermitian);
+DE_API int de_dots_d(de_problem *h, const de_complex *bras_d, const de_complex *kets_d,
+                     int64_t size, int nbra, int nket, de_complex *out_host, int hermitian);
+
+/* EXPECTS(j) = <psi_j|H|psi_j>/<psi_j|psi_j> (Hermitian; c-product when
+ * cshiftopt).  GET_EXPECTS hammod.F90:1261-1301. */
+DE_API int de_get_expects(de_problem *h, const de_complex *psi, int nvec, int cshiftopt,
+                          de_complex *expects);
+
+/* ---- eigensolver: GPLMR_EIG ----------------------------------------- */
+
+/* Block GPLMR with harmonic projection and the BASIC inner solve.
+ * Replaces GPLMR_EIG(HAM,PARAMS,MPIDATA,GMSOLVER,X,E,M,MB,SIGMA,NEV,NS,
+ * MAXIT,TOL,PRECONDITIONER,OUTMODULUS) gplmr.F90:9-374.  x is X(M,MB,NEV)
+ * in/out (start vectors in, Ritz vectors out), e receives NEV eigenvalues.
+ * outmodulus > 0 prints the reference's progress lines to stdout every
+ * outmodulus iterations; 0 is silent.  stats may be NULL. */
+DE_API int de_gplmr_eig(de_problem *h, de_complex *x, de_complex *e, int64_t m, int64_t mb,
+                        de_complex sigma, int nev, int ns, int maxit, double tol,
+                        const de_gmres *gm, int outmodulus, de_stats *stats);
+DE_API int de_gplmr_eig_d(de_problem *h, de_complex *x_d, de_complex *e, int64_t m, int64_t mb,
+                          de_complex sigma, int nev, int ns, int maxit, double tol,
+                          const de_gmres *gm, int outmodulus, de_stats *stats);
+
+/* ---- configuration: Input.Inp namelists + command-line keys ---------- */
+
+/* Everything get_input/get_args (input.F90:143-362) can set. */
+typedef struct {
+    de_params params;
+    de_gmres gmres;
+    int writevecs, readvecs;
+    char invecfile[300], outvecfile[300];
+    int numorbs, singlet, numskip;
+    int outmodulus, takerealpart, hermopt, cshiftopt;
+    int gplmr_nev, gplmr_ns, gplmr_maxit;
+    double gplmr_tol;
+    de_complex gplmr_shift;
+    int kdim, lanblocksize, check;
+    double lantol;
+} de_input;
+
+/* Defaults of input.F90:1-124 for every field. */
+DE_API void de_input_default(de_input *in);
+
+/* Read the &main &grid &molecule &lanczos &gmres &orbitals &gplmr
+ * namelists from path (a missing file leaves the defaults, as the
+ * reference does), then apply argv keys (N= Shift= Outfile= Infile=
+ * NoPetsc Petsc Theta= R= Delta= Nev= Norbs= Gptol= Skip= Gmtol= Iter=
+ * Read Takereal Notakereal Sing Trip).  argv may be NULL. */
+DE_API int de_read_input(const char *path, int argc, const char *const *argv, de_input *in);
+
+/* The Inp=<file> argument of get_inputfile (input.F90:257-276), or
+ * "Input.Inp" when absent.  buf receives at most len bytes. */
+DE_API int de_input_file_arg(int argc, const char *const *argv, char *buf, size_t len);
+
+/* ---- eigenvector files (utils.F90:82-198) ---------------------------- */
+
+/* Write NUM vectors of M x M complex to a Fortran unformatted sequential
+ * file: header record (int32 M, int32 NUM, int64 16*M*M), then one record
+ * per vector, 4-byte record markers with gfortran sub-records beyond 2 GiB. */
+DE_API int de_write_vectors(const char *path, int64_t m, int num, const de_complex *psi);
+
+/* Read num vectors into a grid of M = (2N+1)^3 points.  A file written for
+ * another odd grid is zero-padded or cropped about the centre in all six
+ * coordinates (SIXD_FIX utils.F90:186-198). */
+DE_API int de_read_vectors(const char *path, int64_t m, int num, de_complex *psi);
+
+/* Header of an eigenvector file: its M and number of vectors. */
+DE_API int de_vectors_header(const char *path, int64_t *m, int *num);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DOUBLYEXCITED_B200_H */

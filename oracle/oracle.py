@@ -1,0 +1,567 @@
+"""CPU oracle for doublyexcited's two-electron matvec and GPLMR eigensolver.
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py``'s cpu_baseline / ``--impl reference`` arm may import this module,
+and only as the checker (or as the timed CPU restatement of the reference).
+The product package never imports it.
+
+It restates, loop for loop where it matters, the Fortran reference
+(paths relative to ``complexscale-djhnow/code/``):
+
+* operator set-up: ``INIT_PARAMETERS`` initmod.F90:15-51, ``INIT_HAMILTONIAN``
+  initmod.F90:174-228, ``KEMATRIX`` hammod.F90:235-260, ``GETINVERSE`` /
+  ``RVECTOR`` / ``TOOTHEIGMULT`` tooth.f90:14-204, ``POTENTIAL1/2``
+  hammod.F90:432-582;
+* the matvec ``HAMMULT`` hammod.F90:19-67 (C loops in ``de_oracle.c``);
+* ``GPLMR_EIG`` gplmr.F90:9-374 with ``SOLVE_GEVP``/``EIGSORT``
+  gplmr.F90:395-439,640-660 and ``PRECBLOCK``/``PRECBLOCK_BASIC``
+  gplmr.F90:466-502,674-770;
+* the block ops ``normalize``/``crossmult_diag``/``colnorms``/``crossmult``/
+  ``cholQR`` lamod.f90:21-180;
+* the inner solve ``basicblocklansolve``/``harm_orthog_oneblock``/
+  ``fast_harmritz_setup``/``myhgramschmidt_many``
+  harmonic_ritz_small.F90:28-324 and ``gen_cmatsub`` hr_eigen.f90:223-291;
+* ``GET_EXPECTS`` hammod.F90:1261-1301 and the shift rule
+  doublyexcited.F90:214-219.
+
+Dense LAPACK calls go to the same routines the reference calls (``dsyev``,
+``zggev``, ``zgesdd``, ``zpotrf``, ``ztrsm``) through scipy's LAPACK.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.linalg as sla
+import scipy.linalg.blas as sblas
+import scipy.linalg.lapack as slapack
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build() -> str:
+    """Compile ``de_oracle.c`` into ``oracle/_build/libde_oracle.so``."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return os.path.join(_HERE, "_build", "libde_oracle.so")
+
+
+def lib() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "_build", "libde_oracle.so")
+        src = os.path.join(_HERE, "de_oracle.c")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            build()
+        L = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        L.or_kematrix.argtypes = [ctypes.c_int, ctypes.c_double, P]
+        L.or_rvector.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, P, P]
+        L.or_tootheigmult.argtypes = [P, P, P, ctypes.c_int]
+        L.or_potential1.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, P, P]
+        L.or_potential2.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, P, P]
+        L.or_hammult2.argtypes = [ctypes.c_int, P, P, P, P, P, P]
+        L.or_hammult1.argtypes = [ctypes.c_int, P, P, P, P]
+        for f in (L.or_kematrix, L.or_rvector, L.or_tootheigmult, L.or_potential1,
+                  L.or_potential2, L.or_hammult2, L.or_hammult1):
+            f.restype = None
+        _LIB = L
+    return _LIB
+
+
+def _p(a: np.ndarray) -> ctypes.c_void_p:
+    assert a.flags["F_CONTIGUOUS"] or a.ndim == 1
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+# --------------------------------------------------------------------------
+# set-up
+
+
+def kematrix(nn: int, delta: float) -> np.ndarray:
+    """Real sinc-DVR kinetic matrix, KEMATRIX hammod.F90:235-260."""
+    t = np.zeros((nn, nn), order="F")
+    lib().or_kematrix(nn, float(delta), _p(t))
+    return t
+
+
+def getinverse(nout: int, nbig: int, nsmall: int, delta: float) -> np.ndarray:
+    """Regularised inverse-Laplacian table TINV on (-nout..nout)^3.
+
+    GETINVERSE tooth.f90:14-101: R = delta^3/|r| on the big grid, TR = -T R
+    on the small grid (RVECTOR :106-172), TR(0,0,0) += 2 pi, solve
+    T_3D Q = TR in the eigenbasis of the 1-D T (DSYEV('V','U'), LWORK=6*NS),
+    TINV = R + Q on the small grid, cropped to +-nout.
+    """
+    if nbig < nout:
+        raise ValueError("nbig lt nout")
+    nb, ns = 2 * nbig + 1, 2 * nsmall + 1
+    r = np.zeros((nb, nb, nb), order="F")
+    tr = np.zeros((ns, ns, ns), order="F")
+    lib().or_rvector(nbig, nsmall, float(delta), _p(r), _p(tr))
+    tr[nsmall, nsmall, nsmall] += 2 * math.pi
+    pi = 4.0 * math.atan(1.0)
+    idx = np.arange(-nsmall, nsmall + 1)
+    d = idx[:, None] - idx[None, :]
+    with np.errstate(divide="ignore"):
+        t = np.where(d == 0, (pi / delta) ** 2 / 6.0,
+                     np.where(d % 2 == 0, 1.0, -1.0) / (delta ** 2 * d.astype(float) ** 2))
+    e, w, info = slapack.dsyev(np.asfortranarray(t), compute_v=1, lower=0, lwork=6 * ns)
+    if info != 0:
+        raise RuntimeError(f"dsyev info={info}")
+    w = np.asfortranarray(w)
+    wt = np.asfortranarray(w.T)
+    eigs = e[:, None, None] + e[None, :, None] + e[None, None, :]
+    qq = np.zeros((ns, ns, ns), order="F")
+    lib().or_tootheigmult(_p(tr), _p(qq), _p(wt), ns)
+    qq = np.asfortranarray(qq / eigs)
+    q = np.zeros((ns, ns, ns), order="F")
+    lib().or_tootheigmult(_p(qq), _p(q), _p(w), ns)
+    lo, hi = nbig - nsmall, nbig + nsmall + 1
+    r[lo:hi, lo:hi, lo:hi] += q
+    return np.asfortranarray(r[nbig - nout:nbig + nout + 1, nbig - nout:nbig + nout + 1,
+                               nbig - nout:nbig + nout + 1])
+
+
+@dataclass
+class Params:
+    """Grid/physics parameters (PARAMETERS, structs.F90:28-57)."""
+
+    n: int
+    delta: float = 2.0
+    theta: float = 0.2
+    charge: float = 2.0
+    nsmall: int = 22
+    tfactor: int = 4
+
+    @property
+    def nn(self) -> int:
+        return 2 * self.n + 1
+
+    @property
+    def m(self) -> int:
+        return self.nn ** 3
+
+    @property
+    def scale(self) -> complex:
+        return complex(math.cos(self.theta), math.sin(self.theta))
+
+
+@dataclass
+class Hamiltonian:
+    """Operator data (HAMILTONIAN, structs.F90:87-102) for NELEC = 1 or 2."""
+
+    params: Params
+    nelec: int
+    t_real: np.ndarray
+    tinv: np.ndarray
+    t: np.ndarray = field(repr=False)
+    v: np.ndarray = field(repr=False)
+    _w: np.ndarray | None = field(default=None, repr=False)
+    _z: np.ndarray | None = field(default=None, repr=False)
+    calls: int = 0
+
+    @property
+    def dim(self) -> int:
+        return self.params.m ** self.nelec
+
+    def matvec(self, x: np.ndarray) -> np.ndarray:
+        """HAMMULT hammod.F90:19-67 (NP = 1)."""
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        assert x.shape == (self.dim,)
+        y = np.empty_like(x)
+        self.calls += 1
+        if self.nelec == 2:
+            if self._w is None:
+                self._w = np.empty(self.dim, np.complex128)
+                self._z = np.empty(self.dim, np.complex128)
+            lib().or_hammult2(self.params.nn, _p(self.t), _p(self.v), _p(x), _p(y),
+                              _p(self._w), _p(self._z))
+        else:
+            lib().or_hammult1(self.params.nn, _p(self.t), _p(self.v), _p(x), _p(y))
+        return y
+
+    def matblock(self, x: np.ndarray) -> np.ndarray:
+        """MATBLOCK gplmr.F90:443-462: one HAMMULT per column."""
+        out = np.empty_like(x)
+        for j in range(x.shape[1]):
+            out[:, j] = self.matvec(x[:, j])
+        return out
+
+
+_TINV_CACHE: dict = {}
+
+
+def tinv_table(p: Params) -> np.ndarray:
+    key = (p.nn, p.tfactor * p.nsmall, p.nsmall, p.delta)
+    if key not in _TINV_CACHE:
+        _TINV_CACHE[key] = getinverse(p.nn, p.nsmall * p.tfactor, p.nsmall, p.delta)
+    return _TINV_CACHE[key]
+
+
+def init_hamiltonian(p: Params, nelec: int = 2) -> Hamiltonian:
+    """INIT_HAMILTONIAN initmod.F90:174-228 with the nucleus on the grid."""
+    t_real = kematrix(p.nn, p.delta)
+    t = np.asfortranarray(t_real / p.scale ** 2)
+    tinv = tinv_table(p)
+    if nelec == 1:
+        v = np.zeros(p.m)
+        lib().or_potential1(p.n, float(p.delta), float(p.charge), _p(tinv), _p(v))
+    elif nelec == 2:
+        v = np.zeros(p.m * p.m)
+        lib().or_potential2(p.n, float(p.delta), float(p.charge), _p(tinv), _p(v))
+    else:
+        raise ValueError("nelec must be 1 or 2")
+    v = v / p.scale
+    return Hamiltonian(p, nelec, t_real, tinv, t, v.astype(np.complex128))
+
+
+def dense_one_electron(h: Hamiltonian) -> np.ndarray:
+    """Dense one-electron H = T(x)1(x)1 + 1(x)T(x)1 + 1(x)1(x)T + diag(V)."""
+    assert h.nelec == 1
+    nn = h.params.nn
+    eye = np.eye(nn)
+    t = h.t
+    hk = (np.kron(np.kron(eye, eye), t) + np.kron(np.kron(eye, t), eye)
+          + np.kron(np.kron(t, eye), eye))
+    return hk + np.diag(h.v)
+
+
+# --------------------------------------------------------------------------
+# block operations (lamod.f90)
+
+
+def hdot(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Hermitian cross products A^H B (crossmult, lamod.f90:106-125)."""
+    return a.conj().T @ b
+
+
+def cdot(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Unconjugated c-products A^T B (MPIDOT, hammod.F90:361-380)."""
+    return a.T @ b
+
+
+def colnorms(x: np.ndarray) -> np.ndarray:
+    """sqrt(diag(X^H X)) via ddot on the interleaved reals (lamod.f90:78-102)."""
+    return np.sqrt(np.einsum("ij,ij->j", x.real, x.real) + np.einsum("ij,ij->j", x.imag, x.imag))
+
+
+class CholeskyBreakdown(RuntimeError):
+    pass
+
+
+def cholqr(x: np.ndarray) -> np.ndarray:
+    """In-place Cholesky QR, lamod.f90:128-180: R = chol(X^H X) upper,
+    X <- X R^{-1} (ztrsm 'R','U','N','N').  Returns R."""
+    g = hdot(x, x)
+    if np.sum(np.abs(g)) == 0.0:
+        r = g
+    else:
+        r, info = slapack.zpotrf(g, lower=0, clean=1)
+        if info != 0:
+            raise CholeskyBreakdown(f"Cholesky failed {info}")
+    x[:] = trsm_right_upper(x, r)
+    return r
+
+
+def trsm_right_upper(x: np.ndarray, r: np.ndarray) -> np.ndarray:
+    """X R^{-1} for upper triangular R (ztrsm 'R','U','N','N')."""
+    return sblas.ztrsm(1.0, r, x, side=1, lower=0, trans_a=0, diag=0)
+
+
+# --------------------------------------------------------------------------
+# inner solve (harmonic_ritz_small.F90)
+
+
+def gen_cmatsub_sqrt(a: np.ndarray, tol: float = 0.0):
+    """gen_cmatsub flag=2, hr_eigen.f90:223-291: SVD A = U S V^H (zgesdd),
+    returns (V S^{-1/2} U^H, V S^{1/2} U^H)."""
+    n = a.shape[0]
+    u, s, vt, info = slapack.zgesdd(np.asfortranarray(a.copy()), compute_uv=1, full_matrices=1)
+    if info != 0:
+        raise RuntimeError(f"zgesdd info={info}")
+    sv = s.copy()
+    for k in range(n):
+        if sv[k] != 0.0:
+            if sv[k] < tol * s[0]:
+                sv[k] = 1.0 / tol / s[0]
+            else:
+                sv[k] = 1.0 / sv[k]
+    sv = np.sqrt(sv)
+    ssave = np.sqrt(s)
+    v = vt.conj().T
+    uh = u.conj().T
+    return (v * sv[None, :]) @ uh, (v * ssave[None, :]) @ uh
+
+
+class OrthoCheckFailed(RuntimeError):
+    pass
+
+
+def basicblocklansolve(x: np.ndarray, order: int, maxiter: int, sigma: complex, mult):
+    """Fixed-order block min-residual approximation of (H - sigma)^{-1} X.
+
+    basicblocklansolve harmonic_ritz_small.F90:258-324 with
+    harm_orthog_oneblock :161-244 and fast_harmritz_setup :86-158 (both
+    multiplication callbacks are the same unshifted H, gplmr.F90:700-701).
+    """
+    n, nblk = x.shape
+    if order <= 0:
+        raise ValueError("ORDERERROR")
+    if order * nblk > maxiter:
+        raise ValueError("Order*lanblocknum is greater than lansize")
+    thisdim = min(maxiter, order * nblk)
+    # harm_orthog_oneblock
+    v1 = x.copy()
+    w0 = mult(v1) - sigma * v1
+    g = hdot(w0, w0)
+    ginv, gsq = gen_cmatsub_sqrt(g, 0.0)
+    v1 = v1 @ ginv.conj().T
+    w1 = mult(v1) - sigma * v1
+    chk = hdot(w1, w1) - np.eye(nblk)
+    if np.any(np.abs(chk) > 1e-10):
+        raise OrthoCheckFailed("AACK DOTS")
+    # fast_harmritz_setup
+    lv = np.zeros((n, nblk, order), np.complex128, order="F")
+    lq = np.zeros((n, nblk, order), np.complex128, order="F")
+    for io in range(order):
+        nb_here = nblk
+        if (io + 1) * nblk >= maxiter:
+            nb_here = maxiter - io * nblk
+        if io == 0:
+            lv[:, :, 0] = v1
+        else:
+            lv[:, :nb_here, io] = mult(lv[:, :nb_here, io - 1])
+        lq[:, :nb_here, io] = mult(lv[:, :nb_here, io]) - sigma * lv[:, :nb_here, io]
+        for i in range(nb_here):
+            m = io * nblk + i
+            prev_q = lq.reshape(n, nblk * order, order="F")[:, :m]
+            prev_v = lv.reshape(n, nblk * order, order="F")[:, :m]
+            q = lq[:, i, io].copy()
+            v = lv[:, i, io].copy()
+            for _ in range(2):
+                if m:
+                    dots = prev_q.conj().T @ q
+                    q = q - prev_q @ dots
+                    v = v - prev_v @ dots
+                nrm = np.vdot(q, q)
+                nrm = math.sqrt(abs(nrm))
+                q = q / nrm
+                v = v / nrm
+            lq[:, i, io] = q
+            lv[:, i, io] = v
+    qf = lq.reshape(n, nblk * order, order="F")
+    vf = lv.reshape(n, nblk * order, order="F")
+    lanham = hdot(qf, vf)
+    rhs = np.zeros((order * nblk, nblk), np.complex128)
+    rhs[:nblk, :] = gsq
+    solve = lanham[:thisdim, :thisdim] @ rhs[:thisdim]
+    return vf[:, :thisdim] @ solve
+
+
+# --------------------------------------------------------------------------
+# GPLMR (gplmr.F90)
+
+
+@dataclass
+class GplmrResult:
+    e: np.ndarray
+    x: np.ndarray
+    iterations: int
+    residuals: np.ndarray
+    history: list
+    matvecs: int
+
+
+def solve_gevp(kp: np.ndarray, mp: np.ndarray, k: int, nev: int) -> np.ndarray:
+    """SOLVE_GEVP gplmr.F90:395-439: ZGGEV('N','V') on the leading k x k
+    pencil, sort |alpha/beta| ascending (EIGSORT :640-660, first minimum on
+    ties), return the nev right eigenvectors (k x nev)."""
+    a = np.asfortranarray(kp[:k, :k].copy())
+    b = np.asfortranarray(mp[:k, :k].copy())
+    alpha, beta, vl, vr, work, info = slapack.zggev(a, b, compute_vl=0, compute_vr=1,
+                                                    lwork=10 * max(1, 2 * k))
+    if info != 0:
+        raise RuntimeError("SOLVE OF THE PROJECTED EIGENVALUE PROBLEM FAILED")
+    lam = np.abs(alpha / beta)
+    y = lam.copy()
+    mx = y.max()
+    idx = []
+    for _ in range(nev):
+        i = int(np.argmin(y))
+        idx.append(i)
+        y[i] = mx + 1
+    return vr[:, idx]
+
+
+def gplmr_eig(h: Hamiltonian, x0: np.ndarray, sigma: complex, ns: int = 5, maxit: int = 100,
+              tol: float = 1e-7, order: int = 5, compat_first_column_only: bool = False,
+              max_inner_iter: int | None = None, verbose: bool = False) -> GplmrResult:
+    """GPLMR_EIG gplmr.F90:9-374 with the BASIC preconditioner."""
+    if max_inner_iter is None:
+        max_inner_iter = order
+    calls0 = h.calls
+    x = np.array(x0, dtype=np.complex128, order="F", copy=True)
+    d, nev = x.shape
+    ldr = ns * nev
+    nproj = (3 + ns) * nev
+
+    def precblock(blk: np.ndarray) -> np.ndarray:
+        if max_inner_iter == 1:
+            return h.matblock(blk)
+
+        def mult(v: np.ndarray) -> np.ndarray:
+            if compat_first_column_only:
+                out = np.zeros_like(v)
+                out[:, 0] = h.matvec(v[:, 0])
+                return out
+            return h.matblock(v)
+
+        return basicblocklansolve(blk, max_inner_iter, h.params.m ** 2, sigma, mult)
+
+    x /= colnorms(x)[None, :]
+    ax = h.matblock(x)
+    e = np.einsum("ij,ij->j", x.conj(), ax)
+    w = ax - x * e[None, :]
+    resnrm = colnorms(w)
+    maxres = resnrm.max()
+    it = 1
+    p = np.zeros_like(x)
+    ap = np.zeros_like(x)
+    s = np.zeros((d, ldr), np.complex128, order="F")
+    as_ = np.zeros((d, ldr), np.complex128, order="F")
+    hist = []
+    while it <= maxit and maxres > tol:
+        r = cholqr(x)
+        ax = trsm_right_upper(ax, r)
+        if max_inner_iter > 0:
+            w = precblock(w)
+        r = hdot(x, w)
+        w = w - x @ r
+        cholqr(w)
+        aw = h.matblock(w)
+        if ns > 0:
+            s1 = aw - w * e[None, :]
+            if max_inner_iter > 0:
+                s1 = precblock(s1)
+            s1 = s1 - x @ hdot(x, s1)
+            s1 = s1 - w @ hdot(w, s1)
+            cholqr(s1)
+            s[:, :nev] = s1
+            as_[:, :nev] = h.matblock(s1)
+            for l in range(2, ns + 1):
+                j1, j2 = (l - 1) * nev, l * nev
+                sl = as_[:, j1 - nev:j1] - s[:, j1 - nev:j1] * e[None, :]
+                if max_inner_iter > 0:
+                    sl = precblock(sl)
+                sl = sl - x @ hdot(x, sl)
+                sl = sl - w @ hdot(w, sl)
+                sl = sl - s[:, :j1] @ hdot(s[:, :j1], sl)
+                cholqr(sl)
+                s[:, j1:j2] = sl
+                as_[:, j1:j2] = h.matblock(sl)
+        if it > 1:
+            r = hdot(x, p)
+            p = p - x @ r
+            ap = ap - ax @ r
+            r = hdot(w, p)
+            p = p - w @ r
+            ap = ap - aw @ r
+            r = hdot(s, p)
+            p = p - s @ r
+            ap = ap - as_ @ r
+            r = cholqr(p)
+            ap = trsm_right_upper(ap, r)
+        asx = ax - sigma * x
+        asw = aw - sigma * w
+        ass = as_ - sigma * s
+        if it > 1:
+            asp = ap - sigma * p
+            bra = np.concatenate([asx, asw, ass, asp], axis=1)
+            ket = np.concatenate([x, w, s, p], axis=1)
+            k = nproj
+        else:
+            bra = np.concatenate([asx, asw, ass], axis=1)
+            ket = np.concatenate([x, w, s], axis=1)
+            k = nproj - nev
+        kp = hdot(bra, bra)
+        mp = hdot(bra, ket)
+        vr = solve_gevp(kp, mp, k, nev)
+        cx = vr[:nev]
+        cw = vr[nev:2 * nev]
+        cs = vr[2 * nev:2 * nev + ldr]
+        if it > 1:
+            cp = vr[2 * nev + ldr:nproj]
+            p = p @ cp
+            ap = ap @ cp
+        else:
+            p = np.zeros_like(x)
+            ap = np.zeros_like(x)
+        p = p + s @ cs
+        ap = ap + as_ @ cs
+        p = p + w @ cw
+        ap = ap + aw @ cw
+        x = x @ cx + p
+        ax = ax @ cx + ap
+        nrm = colnorms(x)
+        x = x / nrm[None, :]
+        ax = ax / nrm[None, :]
+        e = np.einsum("ij,ij->j", x.conj(), ax)
+        w = ax - x * e[None, :]
+        resnrm = colnorms(w)
+        maxres = resnrm.max()
+        hist.append((it, e.copy(), resnrm.copy()))
+        if verbose:
+            print(f"ITERATION {it:5d}", " ".join(f"{z.real:.12f}{z.imag:+.12f}i" for z in e),
+                  f"ERR {maxres:.2e}", flush=True)
+        it += 1
+    return GplmrResult(e, x, it - 1, resnrm, hist, h.calls - calls0)
+
+
+def get_expects(h: Hamiltonian, psi: np.ndarray, cshiftopt: bool = False) -> np.ndarray:
+    """GET_EXPECTS hammod.F90:1261-1301 (Hermitian quotients by default)."""
+    out = []
+    for j in range(psi.shape[1]):
+        hp = h.matvec(psi[:, j])
+        if cshiftopt:
+            out.append(np.dot(psi[:, j], hp) / np.dot(psi[:, j], psi[:, j]))
+        else:
+            out.append(np.vdot(psi[:, j], hp) / np.vdot(psi[:, j], psi[:, j]))
+    return np.array(out)
+
+
+def gplmr_shift(expects: np.ndarray, nev: int, takerealpart: bool = True) -> complex:
+    """doublyexcited.F90:214-219."""
+    s = complex(np.sum(expects[:nev]) / nev)
+    return complex(s.real, 0.0) if takerealpart else s
+
+
+# --------------------------------------------------------------------------
+# seeded start vectors
+
+
+def seeded_start(p: Params, nev: int, seed: int, spin: str = "singlet") -> np.ndarray:
+    """Complex-Gaussian columns (N(0,1)+iN(0,1))/sqrt(2), exchange
+    symmetrised X <- (X +- X^T)/sqrt(2) in (p,q), unit Hermitian norm."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    m = p.m
+    out = np.empty((m * m, nev), np.complex128, order="F")
+    sgn = 1.0 if spin == "singlet" else -1.0
+    for j in range(nev):
+        z = (rng.standard_normal((m, m)) + 1j * rng.standard_normal((m, m))) / math.sqrt(2.0)
+        z = (z + sgn * z.T) / math.sqrt(2.0)
+        col = z.reshape(-1, order="F")
+        out[:, j] = col / np.linalg.norm(col)
+    return out
+
+
+def seeded_vectors(dim: int, count: int, seed: int) -> np.ndarray:
+    """Plain complex-Gaussian columns (N(0,1)+iN(0,1))/sqrt(2)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    re = rng.standard_normal((count, dim))
+    im = rng.standard_normal((count, dim))
+    return np.asfortranarray(((re + 1j * im) / math.sqrt(2.0)).T)

@@ -1,0 +1,164 @@
+"""Regenerate the golden fixtures in tests/golden/ from the CPU oracle.
+
+    python tests/golden/make_golden.py [--only NAME ...] [--skip-slow]
+
+Every fixture is produced by the oracle (``oracle/oracle.py`` +
+``oracle/de_oracle.c``), a CPU restatement of the reference's Fortran.  The
+oracle itself is pinned against the reference's own run logs (see
+``heplus_n5.json``: the one-electron spectrum at N=5 printed by the reference
+in CSCALE-WORK/Outs/Out.S.N5:50-64, and ``gplmr_n5_nev1.json``: the
+two-electron resonance of Out.S.N5:147).  Inputs are seeded (numpy PCG64), so
+the script is deterministic.  The N=5 eigensolve takes ~12 minutes on 8
+cores; ``--skip-slow`` leaves it alone.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import oracle as O  # noqa: E402
+
+# One-electron (He+) eigenvalues printed by the reference at N=5, DELTA=2,
+# THETA=0.2 (CSCALE-WORK/Outs/Out.S.N5:50-64, "COMPUTED EIGENVALUES").
+HEPLUS_N5_LOG = [
+    (-1.474195629488970, 0.148077368771954),
+    (-0.457639485991862, 0.029277793106154),
+    (-0.439148582390532, 0.026689746037529),
+    (-0.439148582390528, 0.026689746037529),
+    (-0.439148582390526, 0.026689746037528),
+    (-0.239538038079970, -0.016869829611477),
+    (-0.239538038073564, -0.016869829613176),
+    (-0.219636044640111, 0.002966582358558),
+    (-0.219636021432998, 0.002966570762096),
+    (-0.219636021336936, 0.002966570760415),
+    (-0.206711291449513, 0.007892070211062),
+    (-0.197841608078243, 0.006177361204672),
+    (-0.197839764151099, 0.006178834410508),
+    (-0.197839764101399, 0.006178834223103),
+]
+
+# Two-electron singlet resonance printed by the reference (FINAL EIGVALS).
+RESONANCE_LOG = {
+    "n5": (-0.713154142874, 0.035227459486),   # Out.S.N5:147, residual 7.99e-8
+    "n6_basic": (-0.713140520365, 0.035275084711),  # Out.S.D2d0.T0.2d0.N6.petsc:97
+    "n6_petsc": (-0.713140523217, 0.035275093419),  # Out.S.D2d0.T0.2d0.N6.nopetsc:96
+    "n9": (-0.713160220734, 0.035265681394),   # Out.S.D2d0.T0.2d0.N9.nopetsc.120core:98
+    "n13": (-0.713167246801, 0.035266996014),  # Out.S.D2d0.T0.2d0.N13.nopetsc.120core:98
+}
+
+
+def _c(z):
+    return [float(np.real(z)), float(np.imag(z))]
+
+
+def heplus_n5():
+    p = O.Params(n=5, delta=2.0, theta=0.2)
+    h = O.init_hamiltonian(p, nelec=1)
+    ev = np.linalg.eigvals(O.dense_one_electron(h))
+    ev = ev[np.argsort(ev.real)][:14]
+    return {"params": {"n": 5, "delta": 2.0, "theta": 0.2, "charge": 2.0},
+            "oracle": [_c(z) for z in ev], "reference_log": [list(z) for z in HEPLUS_N5_LOG]}
+
+
+def hammult_fixture(n, theta, seed, full):
+    p = O.Params(n=n, delta=2.0, theta=theta)
+    h = O.init_hamiltonian(p, nelec=2)
+    x = O.seeded_vectors(p.m ** 2, 1, seed)[:, 0]
+    y = h.matvec(x)
+    meta = {"n": n, "delta": 2.0, "theta": theta, "charge": 2.0, "seed": seed}
+    if full:
+        return meta, {"x": x, "y": y}
+    rng = np.random.Generator(np.random.PCG64(seed + 1000))
+    idx = np.sort(rng.choice(y.size, 4096, replace=False))
+    return meta, {"idx": idx, "y_idx": y[idx], "y_norm": np.array([np.linalg.norm(y)]),
+                  "y_sum": np.array([y.sum()])}
+
+
+def hammult1_fixture(n, theta, seed):
+    p = O.Params(n=n, delta=2.0, theta=theta)
+    h = O.init_hamiltonian(p, nelec=1)
+    x = O.seeded_vectors(p.m, 2, seed)
+    y = np.stack([h.matvec(x[:, j]) for j in range(2)], axis=1)
+    return {"n": n, "delta": 2.0, "theta": theta, "seed": seed}, {"x": x, "y": y}
+
+
+def gplmr_fixture(n, theta, sigma, nev, compat, maxit, tol, seed=0, spin="singlet"):
+    p = O.Params(n=n, delta=2.0, theta=theta)
+    h = O.init_hamiltonian(p, nelec=2)
+    x0 = O.seeded_start(p, nev, seed, spin)
+    t0 = time.time()
+    head = {
+        "params": {"n": n, "delta": 2.0, "theta": theta, "charge": 2.0},
+        "start": {"kind": "seeded_start", "seed": seed, "spin": spin, "nev": nev},
+        "solver": {"sigma": _c(sigma), "ns": 5, "order": 5, "maxit": maxit, "tol": tol,
+                   "compat_first_column_only": bool(compat)},
+    }
+    try:
+        r = O.gplmr_eig(h, x0, sigma, ns=5, maxit=maxit, tol=tol, order=5, compat_first_column_only=compat)
+    except O.OrthoCheckFailed as e:
+        # With NEV > 1 the first-column-only product of the reference's
+        # allhmultsub is not linear in the block, so harm_orthog_oneblock's
+        # self-check fails and the reference STOPs ("AACK DOTS").
+        head["error"] = {"kind": "OrthoCheckFailed", "message": str(e)}
+        return head
+    return {
+        "params": {"n": n, "delta": 2.0, "theta": theta, "charge": 2.0},
+        "start": {"kind": "seeded_start", "seed": seed, "spin": spin, "nev": nev},
+        "solver": {"sigma": _c(sigma), "ns": 5, "order": 5, "maxit": maxit, "tol": tol,
+                   "compat_first_column_only": bool(compat)},
+        "iterations": r.iterations,
+        "matvecs_reference": r.matvecs,
+        "e": [_c(z) for z in r.e],
+        "residuals": [float(v) for v in r.residuals],
+        "history": [{"it": it, "e": [_c(z) for z in e], "res": [float(v) for v in res]} for it, e, res in r.history],
+        "oracle_seconds": time.time() - t0,
+    }
+
+
+FIXTURES = {
+    "heplus_n5": (False, lambda: ("json", heplus_n5())),
+    "hammult_n1": (False, lambda: ("npz", hammult_fixture(1, 0.3, 11, True))),
+    "hammult_n2": (False, lambda: ("npz", hammult_fixture(2, 0.3, 12, True))),
+    "hammult_n3": (False, lambda: ("npz", hammult_fixture(3, 0.35, 13, False))),
+    "hammult_n4": (False, lambda: ("npz", hammult_fixture(4, 0.2, 14, False))),
+    "hammult1_n5": (False, lambda: ("npz", hammult1_fixture(5, 0.2, 15))),
+    "gplmr_n3_nev1": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 1, False, 60, 1e-10))),
+    "gplmr_n3_nev4": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 4, False, 12, 1e-10))),
+    "gplmr_n3_nev4_compat": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 4, True, 12, 1e-10))),
+    "gplmr_n5_nev1": (True, lambda: ("json", gplmr_fixture(5, 0.2, complex(-0.7131541429, 0), 1, False, 60, 1e-9))),
+}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", nargs="*")
+    ap.add_argument("--skip-slow", action="store_true")
+    a = ap.parse_args()
+    for name, (slow, fn) in FIXTURES.items():
+        if a.only and name not in a.only:
+            continue
+        if slow and a.skip_slow:
+            continue
+        t0 = time.time()
+        kind, data = fn()
+        if kind == "json":
+            if name.startswith("gplmr_n5"):
+                data["reference_log"] = {"e": list(RESONANCE_LOG["n5"]), "source": "CSCALE-WORK/Outs/Out.S.N5:147"}
+            with open(os.path.join(HERE, name + ".json"), "w") as f:
+                json.dump(data, f, indent=1)
+        else:
+            meta, arrs = data
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), meta=json.dumps(meta), **arrs)
+        print(f"{name}: {time.time() - t0:.1f}s", flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,123 @@
+"""GPU parity of the GPLMR eigensolver (GPLMR_EIG + PRECBLOCK_BASIC) through
+the C ABI against the CPU oracle's runs from the same seeded start vectors,
+and against the reference's logged N=5 resonance.  Bar: complex resonance
+energies within 1e-10 Hartree of the oracle."""
+import numpy as np
+import pytest
+
+from conftest import load_json
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(de, oracle, g, **kw):
+    p = g["params"]
+    s = g["solver"]
+    st = g["start"]
+    op = oracle.Params(n=p["n"], delta=p["delta"], theta=p["theta"])
+    x0 = oracle.seeded_start(op, st["nev"], st["seed"], st["spin"])
+    with de.Problem(n=p["n"], delta=p["delta"], theta=p["theta"]) as h:
+        return h.gplmr_eig(x0, complex(*s["sigma"]), ns=s["ns"], maxit=kw.get("maxit", s["maxit"]),
+                           tol=s["tol"], max_inner_iter=s["order"],
+                           compat_first_column_only=s["compat_first_column_only"])
+
+
+def _history_check(r, g, tol_e):
+    assert r.iterations == g["iterations"]
+    e = np.array([complex(*z) for z in g["e"]])
+    assert np.max(np.abs(np.sort_complex(r.e) - np.sort_complex(e))) < tol_e
+    assert r.matvecs_reference == g["matvecs_reference"]
+
+
+def test_gplmr_n3_nev1_converged(de, oracle):
+    g = load_json("gplmr_n3_nev1.json")
+    r = _run(de, oracle, g)
+    _history_check(r, g, 1e-10)
+    assert r.converged and r.max_residual <= g["solver"]["tol"]
+
+
+def test_gplmr_n3_nev4_tracks_oracle(de, oracle):
+    """NEV=4 for 12 iterations: the Ritz values agree with the oracle's."""
+    g = load_json("gplmr_n3_nev4.json")
+    r = _run(de, oracle, g)
+    assert r.iterations == g["iterations"]
+    e = np.array([complex(*z) for z in g["e"]])
+    assert np.max(np.abs(np.sort_complex(r.e) - np.sort_complex(e))) < 1e-8
+    assert r.matvecs_reference == g["matvecs_reference"]
+
+
+def test_gplmr_first_column_only_mode_stops_like_the_reference(de, oracle):
+    """With NEV > 1 the reference's allhmultsub multiplies only the first
+    column; the inner solve's orthonormality self-check then fails (the
+    oracle raises, the reference STOPs with "AACK DOTS").  The C ABI
+    returns DE_E_ORTHO."""
+    g = load_json("gplmr_n3_nev4_compat.json")
+    assert g["error"]["kind"] == "OrthoCheckFailed"
+    with pytest.raises(de.DeError) as e:
+        _run(de, oracle, g)
+    assert e.value.status == de.DE_E_ORTHO
+
+
+def test_gplmr_n5_resonance_matches_oracle_and_reference_log(de, oracle):
+    g = load_json("gplmr_n5_nev1.json")
+    r = _run(de, oracle, g)
+    e_or = complex(*g["e"][0])
+    e_log = complex(*g["reference_log"]["e"])
+    assert r.converged
+    assert abs(r.e[0] - e_or) < 1e-10
+    assert abs(r.e[0] - e_log) < 2e-9
+
+
+def test_gplmr_iteration_history_prefix(de, oracle):
+    """The first iterations' Rayleigh quotients track the oracle's."""
+    g = load_json("gplmr_n3_nev1.json")
+    k = 8
+    r = _run(de, oracle, g, maxit=k)
+    e = complex(*g["history"][k - 1]["e"][0])
+    assert abs(r.e[0] - e) < 1e-10
+
+
+def test_petsc_path_is_unsupported(de, oracle):
+    p = oracle.Params(n=2, delta=2.0, theta=0.3)
+    x0 = oracle.seeded_start(p, 1, 0)
+    with de.Problem(n=2, delta=2.0, theta=0.3) as h:
+        with pytest.raises(de.DeError) as e:
+            h.gplmr_eig(x0, -0.78, maxit=2, usepetscflag=0)
+        assert e.value.status == de.DE_E_UNSUPPORTED
+
+
+def test_matvec_accounting(de, oracle):
+    """ICALLED accounting of the reference: per iteration (1+NS)*NEV MATBLOCK
+    products plus (1+NS) PRECBLOCK calls of (2*order+1) products each (NEV
+    columns each in the fixed mode)."""
+    p = oracle.Params(n=2, delta=2.0, theta=0.3)
+    x0 = oracle.seeded_start(p, 2, 0)
+    with de.Problem(n=2, delta=2.0, theta=0.3) as h:
+        r = h.gplmr_eig(x0, -0.78, maxit=3, tol=1e-14)
+        assert r.iterations == 3
+        assert r.matvecs_reference == 2 + 3 * 6 * (2 + 2 * 11)
+        assert r.matvecs == 2 + 3 * 6 * (2 + 2 * 10)
+        r = h.gplmr_eig(x0[:, :1], -0.78, maxit=3, tol=1e-14, compat_first_column_only=True)
+        assert r.matvecs_reference == 1 + 3 * 6 * (1 + 11)  # NEV=1: the mode changes nothing
+
+
+def test_get_expects_and_shift(de, oracle):
+    p = oracle.Params(n=3, delta=2.0, theta=0.2)
+    h = oracle.init_hamiltonian(p, nelec=2)
+    psi = oracle.seeded_start(p, 2, 4)
+    ref = oracle.get_expects(h, psi)
+    ref_c = oracle.get_expects(h, psi, cshiftopt=True)
+    with de.Problem(n=3, delta=2.0, theta=0.2) as g:
+        assert np.max(np.abs(g.get_expects(psi) - ref)) < 1e-12
+        assert np.max(np.abs(g.get_expects(psi, cshiftopt=True) - ref_c)) < 1e-12
+
+
+def test_dots(de, oracle):
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal((100003, 5)) + 1j * rng.standard_normal((100003, 5))
+    b = rng.standard_normal((100003, 70)) + 1j * rng.standard_normal((100003, 70))
+    with de.Problem(n=1, delta=2.0, theta=0.3) as g:
+        h = g.dots(a, b, hermitian=True)
+        c = g.dots(a, b, hermitian=False)
+    assert np.max(np.abs(h - a.conj().T @ b)) < 1e-9
+    assert np.max(np.abs(c - a.T @ b)) < 1e-9

@@ -1,0 +1,143 @@
+"""GPU parity of the matvec (HAMMULT / MATBLOCK) through the C ABI against
+the CPU oracle and the golden fixtures.  Bar: relative 2-norm error <= 1e-12
+(the plain FP64 form must match the reference's matvec to 1e-12)."""
+import numpy as np
+import pytest
+
+from conftest import load_npz, rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+@pytest.mark.parametrize("n,theta", [(1, 0.3), (2, 0.0), (2, 0.35), (3, 0.2), (4, 0.3), (5, 0.2), (6, 0.2)])
+def test_hammult_matches_oracle(de, oracle, n, theta):
+    p = oracle.Params(n=n, delta=2.0, theta=theta)
+    h = oracle.init_hamiltonian(p, nelec=2)
+    x = oracle.seeded_vectors(p.m ** 2, 1, 100 + n)[:, 0]
+    with de.Problem(n=n, delta=2.0, theta=theta) as g:
+        y = g.hammult(x)
+    assert rel_err(y, h.matvec(x)) < TOL
+
+
+@pytest.mark.parametrize("n", [7, 8])
+def test_hammult_matches_oracle_large(de, oracle, n):
+    """N=7,8 (NN=15,17): the shared-memory tilings of the larger grids."""
+    p = oracle.Params(n=n, delta=2.0, theta=0.35)
+    h = oracle.init_hamiltonian(p, nelec=2)
+    x = oracle.seeded_vectors(p.m ** 2, 1, 7)[:, 0]
+    with de.Problem(n=n, delta=2.0, theta=0.35) as g:
+        y = g.hammult(x)
+    assert rel_err(y, h.matvec(x)) < TOL
+
+
+@pytest.mark.parametrize("name", ["hammult_n1.npz", "hammult_n2.npz"])
+def test_hammult_full_golden(de, name):
+    meta, a = load_npz(name)
+    with de.Problem(n=meta["n"], delta=meta["delta"], theta=meta["theta"]) as g:
+        assert rel_err(g.hammult(a["x"]), a["y"]) < TOL
+
+
+@pytest.mark.parametrize("name", ["hammult_n3.npz", "hammult_n4.npz"])
+def test_hammult_sampled_golden(de, oracle, name):
+    meta, a = load_npz(name)
+    p = oracle.Params(n=meta["n"], delta=meta["delta"], theta=meta["theta"])
+    x = oracle.seeded_vectors(p.m ** 2, 1, meta["seed"])[:, 0]
+    with de.Problem(n=meta["n"], delta=meta["delta"], theta=meta["theta"]) as g:
+        y = g.hammult(x)
+    assert rel_err(y[a["idx"]], a["y_idx"]) < TOL
+    assert abs(np.linalg.norm(y) - a["y_norm"][0]) < TOL * a["y_norm"][0]
+
+
+def test_one_electron_golden(de):
+    """NELEC=1 (KEMULT1 + POTENTIAL1), the operator of the He+ pin."""
+    meta, a = load_npz("hammult1_n5.npz")
+    with de.Problem(n=meta["n"], delta=meta["delta"], theta=meta["theta"], nelec=1) as g:
+        y = g.matblock(a["x"])
+    assert rel_err(y, a["y"]) < TOL
+
+
+def test_heplus_ground_state_by_power_free_check(de, oracle):
+    """The GPU one-electron operator reproduces the reference's He+ level:
+    for the oracle's dense eigenvector v of E0, ||H v - E0 v|| is tiny."""
+    p = oracle.Params(n=5, delta=2.0, theta=0.2)
+    h = oracle.init_hamiltonian(p, nelec=1)
+    w, v = np.linalg.eig(oracle.dense_one_electron(h))
+    i = int(np.argmin(w.real))
+    with de.Problem(n=5, delta=2.0, theta=0.2, nelec=1) as g:
+        hv = g.hammult(v[:, i])
+    e_log = complex(-1.474195629488970, 0.148077368771954)
+    assert abs(w[i] - e_log) < 1e-12
+    assert np.linalg.norm(hv - e_log * v[:, i]) < 1e-11
+
+
+def test_matblock_is_columnwise_hammult(de, oracle):
+    p = oracle.Params(n=3, delta=2.0, theta=0.3)
+    x = oracle.seeded_vectors(p.m ** 2, 3, 21)
+    with de.Problem(n=3, delta=2.0, theta=0.3) as g:
+        ax = g.matblock(x)
+        for j in range(3):
+            assert np.array_equal(ax[:, j], g.hammult(x[:, j]))  # deterministic, bitwise
+
+
+def test_size_mismatch_is_an_error(de):
+    import ctypes
+
+    with de.Problem(n=2, delta=2.0, theta=0.3) as g:
+        x = np.zeros(g.dim + 1, np.complex128)
+        y = np.zeros_like(x)
+        s = de.lib().de_hammult(g.handle, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(y.ctypes.data), g.dim + 1)
+        assert s == de.DE_E_SIZE
+        s = de.lib().de_matblock(g.handle, ctypes.c_void_p(x.ctypes.data), ctypes.c_void_p(y.ctypes.data),
+                                 g.m, g.m + 1, 1)
+        assert s == de.DE_E_SIZE
+
+
+def test_device_pointer_api(de, oracle):
+    import torch
+
+    p = oracle.Params(n=4, delta=2.0, theta=0.3)
+    x = oracle.seeded_vectors(p.m ** 2, 2, 9)
+    with de.Problem(n=4, delta=2.0, theta=0.3) as g:
+        ref = g.matblock(x)
+        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        xd = torch.from_numpy(np.ascontiguousarray(x.T)).cuda()
+        yd = torch.empty_like(xd)
+        g.matblock_d(xd.data_ptr(), yd.data_ptr(), 2)
+        y = yd.cpu().numpy().T  # ordered after the kernels on the same stream
+    assert np.array_equal(y, ref)
+
+
+@pytest.mark.parametrize("n", [9, 10])
+def test_full_size_properties(de, n):
+    """At the benchmark sizes (N=9: 753 MB per vector) the oracle is too
+    slow, so check size-independent properties on the device: linearity,
+    complex symmetry x^T H y = y^T H x and electron exchange
+    H(X^T) = (H X)^T."""
+    import torch
+
+    with de.Problem(n=n, delta=2.0, theta=0.35) as g:
+        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        m, dim = g.m, g.dim
+        gen = torch.Generator(device="cuda").manual_seed(5)
+        x = torch.randn(dim, dtype=torch.complex128, device="cuda", generator=gen)
+        y = torch.randn(dim, dtype=torch.complex128, device="cuda", generator=gen)
+        hx = torch.empty_like(x)
+        hy = torch.empty_like(x)
+        g.matblock_d(x.data_ptr(), hx.data_ptr(), 1)
+        g.matblock_d(y.data_ptr(), hy.data_ptr(), 1)
+        a = torch.dot(x, hy)
+        b = torch.dot(y, hx)
+        assert abs(a - b).item() < 1e-12 * abs(a).item()
+        z = 2 * x + 1j * y
+        hz = torch.empty_like(z)
+        g.matblock_d(z.data_ptr(), hz.data_ptr(), 1)
+        err = torch.linalg.norm(hz - (2 * hx + 1j * hy)) / torch.linalg.norm(hz)
+        assert err.item() < 1e-14
+        del y, hy, z, hz
+        xt = x.view(m, m).t().contiguous().view(-1)  # X^T in the reference layout
+        hxt = torch.empty_like(xt)
+        g.matblock_d(xt.data_ptr(), hxt.data_ptr(), 1)
+        err = torch.linalg.norm(hxt - hx.view(m, m).t().contiguous().view(-1)) / torch.linalg.norm(hx)
+        assert err.item() < 1e-13
+        torch.cuda.synchronize()

@@ -1,0 +1,111 @@
+"""The CPU oracle, pinned against the reference's own run logs and an
+independent dense construction.  No GPU."""
+import numpy as np
+import pytest
+
+from conftest import load_json, load_npz, rel_err
+
+
+def test_heplus_spectrum_matches_reference_log(oracle):
+    """He+ at N=5, DELTA=2, THETA=0.2: the dense one-electron spectrum equals
+    the 14 eigenvalues the reference printed (Out.S.N5:50-64).  This pins
+    KEMATRIX, GETINVERSE/TINV, POTENTIAL1 and the 1/SCALE conventions."""
+    g = load_json("heplus_n5.json")
+    p = oracle.Params(n=5, delta=2.0, theta=0.2)
+    h = oracle.init_hamiltonian(p, nelec=1)
+    ev = np.linalg.eigvals(oracle.dense_one_electron(h))
+    ev = ev[np.argsort(ev.real)][:14]
+    log = np.array([complex(a, b) for a, b in g["reference_log"]])
+    # the seven lowest levels (through the first 2p-like multiplet) agree to
+    # the reference's printed digits; the lowest to machine precision
+    assert abs(ev[0] - log[0]) < 1e-13
+    assert np.max(np.abs(ev[:7] - log[:7])) < 1e-10
+    # the upper levels were still converging when the reference's block
+    # Lanczos stopped (error 1.8e-3 at Out.S.N5:48): looser agreement
+    assert np.max(np.abs(ev - log)) < 1e-5
+    assert np.max(np.abs(ev - np.array([complex(*z) for z in g["oracle"]]))) < 1e-12
+
+
+def _dense_two_electron(oracle, n, theta):
+    """Independent construction: H2 = K1 (x) I + I (x) K1 + diag(V2), with K1
+    the one-electron kinetic Kronecker sum and V2 built from TINV directly."""
+    p = oracle.Params(n=n, delta=2.0, theta=theta)
+    h1 = oracle.init_hamiltonian(p, nelec=1)
+    nn = p.nn
+    eye = np.eye(nn)
+    t = h1.t
+    k1 = np.kron(np.kron(eye, eye), t) + np.kron(np.kron(eye, t), eye) + np.kron(np.kron(t, eye), eye)
+    m = p.m
+    km = np.kron(np.eye(m), k1) + np.kron(k1, np.eye(m))
+    tinv = h1.tinv
+    nb = nn
+    coords = np.array([(i - n, j - n, k - n) for k in range(nn) for j in range(nn) for i in range(nn)])
+    a = -2.0 / p.delta ** 3
+    t1 = tinv[coords[:, 0] + nb, coords[:, 1] + nb, coords[:, 2] + nb]
+    d = coords[None, :, :] - coords[:, None, :]  # d[p, q] = r_q - r_p
+    t12 = tinv[d[..., 0] + nb, d[..., 1] + nb, d[..., 2] + nb] / p.delta ** 3
+    v = (a * t1[None, :] + a * t1[:, None] + t12)  # V(p, q)
+    vv = v.reshape(-1, order="F") / p.scale
+    return km + np.diag(vv)
+
+
+def test_oracle_hammult_equals_dense_construction(oracle):
+    p = oracle.Params(n=1, delta=2.0, theta=0.3)
+    h = oracle.init_hamiltonian(p, nelec=2)
+    x = oracle.seeded_vectors(p.m ** 2, 1, 3)[:, 0]
+    hd = _dense_two_electron(oracle, 1, 0.3)
+    assert rel_err(h.matvec(x), hd @ x) < 1e-13
+
+
+def test_operator_symmetries(oracle):
+    """H is complex symmetric (H^T = H) and commutes with electron exchange."""
+    p = oracle.Params(n=3, delta=2.0, theta=0.35)
+    h = oracle.init_hamiltonian(p, nelec=2)
+    x, y = oracle.seeded_vectors(p.m ** 2, 2, 5).T
+    assert abs(x @ h.matvec(y) - y @ h.matvec(x)) < 1e-11 * abs(x @ h.matvec(y))
+    m = p.m
+    xt = x.reshape(m, m, order="F").T.reshape(-1, order="F")
+    hxt = h.matvec(xt)
+    hx_t = h.matvec(x).reshape(m, m, order="F").T.reshape(-1, order="F")
+    assert rel_err(hxt, hx_t) < 1e-13
+
+
+@pytest.mark.parametrize("name", ["hammult_n1.npz", "hammult_n2.npz"])
+def test_oracle_reproduces_full_golden(oracle, name):
+    meta, a = load_npz(name)
+    p = oracle.Params(n=meta["n"], delta=meta["delta"], theta=meta["theta"])
+    h = oracle.init_hamiltonian(p, nelec=2)
+    assert rel_err(h.matvec(a["x"]), a["y"]) < 1e-14
+
+
+@pytest.mark.parametrize("name", ["hammult_n3.npz", "hammult_n4.npz"])
+def test_oracle_reproduces_sampled_golden(oracle, name):
+    meta, a = load_npz(name)
+    p = oracle.Params(n=meta["n"], delta=meta["delta"], theta=meta["theta"])
+    h = oracle.init_hamiltonian(p, nelec=2)
+    x = oracle.seeded_vectors(p.m ** 2, 1, meta["seed"])[:, 0]
+    y = h.matvec(x)
+    assert rel_err(y[a["idx"]], a["y_idx"]) < 1e-14
+    assert abs(np.linalg.norm(y) - a["y_norm"][0]) < 1e-12 * a["y_norm"][0]
+
+
+def test_gplmr_n5_fixture_matches_reference_log():
+    """The oracle's converged N=5 resonance agrees with the reference's logged
+    value (printed at residual 8e-8) to 1e-9 Hartree."""
+    g = load_json("gplmr_n5_nev1.json")
+    e = complex(*g["e"][0])
+    log = complex(*g["reference_log"]["e"])
+    assert g["residuals"][0] < 1e-9
+    assert abs(e - log) < 1e-9
+
+
+def test_oracle_gplmr_small_runs(oracle):
+    """A short GPLMR run on N=2 decreases the residual and keeps the
+    reference's matvec accounting: 1 + iters*(1+NS)*(NEV + NEV*(2*order+1))."""
+    p = oracle.Params(n=2, delta=2.0, theta=0.3)
+    h = oracle.init_hamiltonian(p, nelec=2)
+    x0 = oracle.seeded_start(p, 1, 0)
+    r = oracle.gplmr_eig(h, x0, complex(-0.78, 0), ns=5, maxit=4, tol=1e-14, order=5)
+    assert r.iterations == 4
+    assert r.matvecs == 1 + 4 * 6 * (1 + 11)
+    assert r.history[-1][2][0] < r.history[0][2][0]
