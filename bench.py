@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark: converged helium resonance solves per second on B200.
+
+Workload (default ``solve-n6``): the reference's own logged configuration
+(CSCALE-WORK/Outs/Out.S.D2d0.T0.2d0.N6.petsc: singlet, N=6 so NN=13 points
+per axis and a 4,826,809-dimensional two-electron space, DELTA=2, THETA=0.2,
+GPLMR with NEV=1, NS=5 and the BASIC inner solve of order 5, shift
+-0.7131541429), solved to a residual of 1e-8 (|dE| ~ 1e-9 Hartree) from a
+seeded complex-Gaussian singlet start vector.  One step = one solve.
+
+  value  solves/s with the start vector already in HBM (de_gplmr_eig_d)
+  e2e    solves/s through the C ABI with host buffers (de_gplmr_eig: the
+         start vector is copied host->device and the Ritz vector back)
+  roofline  the dominant kernel, the FP64 matvec (two passes per vector),
+         timed with CUDA events on its stream over the timed region
+  cpu_baseline  the oracle's HAMMULT (the reference's KEMULT2 loop structure
+         in C with OpenMP, all host cores) on a bounded sample of matvecs,
+         converted with the solve's HAMMULT count; block operations are not
+         charged, so it is a lower bound on the CPU solve time
+
+``--impl reference`` runs that CPU path alone (rank 0) and prints its line.
+Multi-GPU: independent replicas (one solve stream per rank, no collective
+on the data path); value = solves of all ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: grid/solver settings; iters_ref = GPLMR iterations to converge
+    # from this seeded start (deterministic; the CPU oracle and the GPU solver
+    # agree), used only by the CPU arm to convert matvec time to solve time.
+    "solve-n6": dict(n=6, delta=2.0, theta=0.2, nev=1, ns=5, order=5, sigma=-0.7131541429, tol=1e-8,
+                     seed=0, spin="singlet", maxit=200, iters_ref=50),
+    "solve-n5": dict(n=5, delta=2.0, theta=0.2, nev=1, ns=5, order=5, sigma=-0.7131541429, tol=1e-9,
+                     seed=0, spin="singlet", maxit=200, iters_ref=52),
+    "solve-n8-nev8": dict(n=8, delta=2.0, theta=0.35, nev=8, ns=5, order=5, sigma=-0.78, tol=1e-7,
+                          seed=2, spin="singlet", maxit=200, iters_ref=None),
+}
+
+
+def hammults_per_solve(w, iters):
+    """The reference's HAMMULT count (ICALLED) for a solve of `iters`
+    iterations: NEV for the start, then per iteration (1+NS) MATBLOCKs of NEV
+    and (1+NS) PRECBLOCK_BASIC calls of (2*order+1) products of NEV."""
+    nev, ns, order = w["nev"], w["ns"], w["order"]
+    return nev + iters * (1 + ns) * (nev + nev * (2 * order + 1))
+
+
+def alg_flops(nn):
+    """Algorithmic FP64 flops of one vector-matvec: 6 axes x NN MACs x 2
+    flops x 2 (re, im) per element, plus the complex potential multiply-add."""
+    return 24 * nn ** 7 + 8 * nn ** 6
+
+
+def alg_bytes(nn):
+    """Read x and write y once, complex128."""
+    return 32 * nn ** 6
+
+
+# dram bytes (read + write) per vector-matvec (pass A + pass B) from the ncu
+# capture summarised in profiles/stream_kernel_n6.md; None until captured.
+NCU_TRAFFIC_PER_VECTOR = {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_peak_tflops(torch):
+    """Measured FP64 dense peak on this GPU: cuBLAS DGEMM 8192^3 (FP64 tensor
+    cores), best of 5 -- the compute denominator of the matvec roofline."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2 * n ** 3 / best / 1e12
+
+
+def cpu_matvec_seconds(w, reps):
+    """Seconds per oracle HAMMULT (C, OpenMP over columns, all host cores)."""
+    from oracle import oracle as O  # CPU baseline only
+
+    p = O.Params(n=w["n"], delta=w["delta"], theta=w["theta"])
+    h = O.init_hamiltonian(p, nelec=2)
+    x = O.seeded_start(p, 1, w["seed"], w["spin"])[:, 0]
+    h.matvec(x)  # warm
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        h.matvec(x)
+    return (time.perf_counter() - t0) / reps, os.cpu_count()
+
+
+def dist_setup():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def run_reference(a, w):
+    rank, world, local = dist_setup()
+    if rank != 0:
+        return 0
+    iters = w["iters_ref"]
+    if iters is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no converged iteration count recorded for this workload"}))
+        return 0
+    nmv = hammults_per_solve(w, iters)
+    for _ in range(a.warmup):
+        cpu_matvec_seconds(w, 1)
+    times = []
+    for _ in range(a.steps):
+        t, cores = cpu_matvec_seconds(w, 2)
+        times.append(t)
+    t_mv = statistics.median(times)
+    solve_s = nmv * t_mv
+    v = 1.0 / solve_s
+    nn = 2 * w["n"] + 1
+    line = {
+        "impl": "reference", "metric": "resonance solves/s", "value": v, "unit": "solves/s", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": solve_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": a.workload, "N": w["n"], "NN": nn, "dim": nn ** 6, "nev": w["nev"], "ns": w["ns"],
+                   "order": w["order"], "theta": w["theta"], "delta": w["delta"], "tol": w["tol"],
+                   "parallelism": "cpu-openmp"},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": f"{2 * a.steps} oracle HAMMULTs at N={w['n']} (C, OpenMP, all cores), "
+                                   f"x {nmv} HAMMULTs per solve ({iters} GPLMR iterations); block ops not charged"},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="solve-n6", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    w = WORKLOADS[a.workload]
+    if a.impl == "reference":
+        return run_reference(a, w)
+
+    import numpy as np
+    import torch
+
+    import doublyexcited_b200 as de
+    from doublyexcited_b200.starts import seeded_start
+
+    rank, world, local = dist_setup()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+
+    def barrier():
+        if pg:
+            pg.barrier()
+
+    nn = 2 * w["n"] + 1
+    prob = de.Problem(n=w["n"], delta=w["delta"], theta=w["theta"], device=local)
+    stream = torch.cuda.current_stream()
+    prob.set_stream(stream.cuda_stream)
+    x0 = seeded_start(prob.m, w["nev"], w["seed"], w["spin"])
+    dim = prob.dim
+    x0_dev = torch.from_numpy(np.ascontiguousarray(x0.T)).to("cuda")  # (nev, dim): columns contiguous
+    x_dev = torch.empty_like(x0_dev)
+    e_host = np.empty(w["nev"], np.complex128)
+
+    import ctypes
+
+    from doublyexcited_b200._lib import check, de_complex, de_gmres, de_stats, lib
+
+    L = lib()
+    gm = de_gmres(w["order"], 1, 1e-3, 0)
+    sig = de_complex(w["sigma"], 0.0)
+
+    def solve_dev():
+        x_dev.copy_(x0_dev)
+        st = de_stats()
+        check(L.de_gplmr_eig_d(prob.handle, ctypes.c_void_p(x_dev.data_ptr()), ctypes.c_void_p(e_host.ctypes.data),
+                               prob.m, dim // prob.m, sig, w["nev"], w["ns"], w["maxit"], w["tol"], ctypes.byref(gm), 0,
+                               ctypes.byref(st)), "de_gplmr_eig_d")
+        return st
+
+    for _ in range(a.warmup):
+        st = solve_dev()
+    torch.cuda.synchronize()
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    prob.set_profiling(True)
+    prob.profile_read()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = L.de_kernel_launches()
+    e0.record(stream)
+    stats = []
+    for _ in range(a.steps):
+        stats.append(solve_dev())
+    e1.record(stream)
+    launches = L.de_kernel_launches() - launches0
+    torch.cuda.synchronize()
+    elapsed = e0.elapsed_time(e1) / 1e3
+    barrier()
+    clocks = sampler.stop()
+    prof = prob.profile_read()
+    prob.set_profiling(False)
+    if pg:
+        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = a.steps * world / elapsed
+    st = stats[-1]
+    e_final = complex(e_host[0])
+
+    # end to end through the host-pointer C ABI (pinned host buffers)
+    x_pin = torch.from_numpy(np.asfortranarray(x0).reshape(-1, order="F").view(np.float64)).pin_memory()
+    x_host = x_pin.numpy().view(np.complex128).reshape(x0.shape, order="F")
+    x_work = torch.empty_like(x_pin).pin_memory()
+    xw = x_work.numpy().view(np.complex128).reshape(x0.shape, order="F")
+    prob.set_stream(0)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(a.steps, 2))
+    for _ in range(e2e_steps):
+        np.copyto(xw, x_host)
+        st2 = de_stats()
+        check(L.de_gplmr_eig(prob.handle, ctypes.c_void_p(xw.ctypes.data), ctypes.c_void_p(e_host.ctypes.data),
+                             prob.m, dim // prob.m, sig, w["nev"], w["ns"], w["maxit"], w["tol"], ctypes.byref(gm), 0,
+                             ctypes.byref(st2)), "de_gplmr_eig")
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if pg:
+        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = e2e_steps * world / t_e2e
+
+    peak = fp64_peak_tflops(torch)
+    mv_ms = prof["pass_a_ms"] + prof["pass_b_ms"]
+    vecs = max(1, prof["vectors"])
+    achieved = alg_flops(nn) * vecs / (mv_ms / 1e3) / 1e12 if mv_ms > 0 else 0.0
+    traffic = NCU_TRAFFIC_PER_VECTOR.get(nn)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        t_mv, cores = cpu_matvec_seconds(w, 3)
+        nmv = st.matvecs_reference
+        cpu = {"value": 1.0 / (nmv * t_mv), "unit": "solves/s", "cores": cores, "kind": "port",
+               "sample": f"3 oracle HAMMULTs at N={w['n']} (C, OpenMP over columns, {cores} threads) "
+                         f"= {t_mv:.3f} s each, x {nmv} HAMMULTs per solve; block ops not charged"}
+
+    if rank == 0:
+        line = {
+            "metric": "resonance solves/s", "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": elapsed / a.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded complex-Gaussian singlet start vector; operator from the reference's physics)",
+            "config": {"workload": a.workload, "N": w["n"], "NN": nn, "dim": dim, "nev": w["nev"], "ns": w["ns"],
+                       "order": w["order"], "theta": w["theta"], "delta": w["delta"], "sigma": w["sigma"],
+                       "tol": w["tol"], "precision": "fp64",
+                       "l2": "inputs larger than L2 (GPLMR workspace "
+                             f"{(17 + 2 * w['order']) * w['nev'] * dim * 16 / 1e9:.1f} GB per solve)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": int(x0.nbytes),
+                    "d2h_bytes_per_step": int(x0.nbytes + e_host.nbytes)},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if peak else None,
+                         "traffic": traffic,
+                         "kernel": "hammult stream_kernel pass A + pass B (FP64), per vector-matvec",
+                         "alg_flops_per_vector": alg_flops(nn), "alg_bytes_per_vector": alg_bytes(nn),
+                         "achieved_gbs_alg": alg_bytes(nn) * vecs / (mv_ms / 1e3) / 1e9 if mv_ms > 0 else None,
+                         "matvec_ms_per_vector": mv_ms / vecs, "pass_a_ms": prof["pass_a_ms"] / vecs,
+                         "pass_b_ms": prof["pass_b_ms"] / vecs,
+                         "peak_source": "FP64 dense peak measured in this run: cuBLAS DGEMM 8192^3 (no FP64 "
+                                        "entry in MEASURED_PEAKS.json)"},
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "solve": {"iterations": st.iterations, "converged": bool(st.converged), "E": [e_final.real, e_final.imag],
+                      "max_residual": st.max_residual, "matvecs": st.matvecs,
+                      "matvecs_reference": st.matvecs_reference, "t_prec_s": st.t_prec_s,
+                      "t_dense_s": st.t_dense_s},
+        }
+        print(json.dumps(line))
+    prob.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -112,11 +112,15 @@ SIGNATURES = {
     "de_strerror": (ctypes.c_char_p, [INT]),
     "de_last_error": (ctypes.c_char_p, []),
     "de_version": (ctypes.c_char_p, []),
+    "de_kernel_launches": (I64, []),
     "de_params_default": (None, [ctypes.POINTER(de_params)]),
     "de_problem_create": (INT, [ctypes.POINTER(de_params), ctypes.POINTER(P)]),
     "de_problem_destroy": (INT, [P]),
     "de_problem_dims": (INT, [P, ctypes.POINTER(INT), ctypes.POINTER(I64), ctypes.POINTER(I64)]),
     "de_set_stream": (INT, [P, P]),
+    "de_set_profiling": (INT, [P, INT]),
+    "de_profile_read": (INT, [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                              ctypes.POINTER(I64), ctypes.POINTER(I64)]),
     "de_hammult": (INT, [P, P, P, I64]),
     "de_hammult_d": (INT, [P, P, P, I64]),
     "de_matblock": (INT, [P, P, P, I64, I64, INT]),

@@ -91,6 +91,18 @@ class Problem:
         stream)."""
         check(lib().de_set_stream(self._h, ctypes.c_void_p(cuda_stream)), "de_set_stream")
 
+    def set_profiling(self, on: bool) -> None:
+        check(lib().de_set_profiling(self._h, int(bool(on))), "de_set_profiling")
+
+    def profile_read(self) -> dict:
+        """Device ms of matvec pass A / pass B, MATBLOCK calls and vectors since
+        the last read (resets)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        c, v = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().de_profile_read(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(v)),
+              "de_profile_read")
+        return {"pass_a_ms": a.value, "pass_b_ms": b.value, "calls": c.value, "vectors": v.value}
+
     # -- operator ---------------------------------------------------------
     def hammult(self, x: np.ndarray) -> np.ndarray:
         x = _block(x, self.dim)[:, 0].copy()

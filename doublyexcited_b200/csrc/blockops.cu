@@ -14,8 +14,14 @@
 #include "de_kernels.h"
 
 #include <algorithm>
+#include <atomic>
 
 namespace de {
+
+static std::atomic<int64_t> g_launches{0};
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
 namespace {
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b)
@@ -26,6 +32,7 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b)
 // ---------------------------------------------------------------- Gram
 
 constexpr int kGramRT = 32;  // rows per smem tile
+constexpr int kSmallBlocks = 296;  // grid of the fused small reductions
 constexpr int kGramTX = 16;  // thread grid 16 x 16
 
 __device__ __forceinline__ double2 col_elem(const ColList &L, int c, int64_t r)
@@ -148,6 +155,7 @@ cudaError_t gram_go(const ColList &L, const ColList &R, int64_t len, int herm, d
         attr[dev] = true;
     }
     gram_partial<TA, TB><<<nblk, 256, smem, st>>>(L, R, len, chunk, herm, work);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -206,6 +214,7 @@ cudaError_t update_go(const UpdList &U, const double2 *c, int ldc, int64_t len, 
     const int64_t want = (len + 255) / 256;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, 148 * 8));
     update_kernel<NOUT><<<blocks, 256, smem, st>>>(U, c, ldc, len);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -323,6 +332,164 @@ __global__ void tables_kernel(int nn, int n, double charge, double delta,
     }
 }
 
+// ---------------------------------------------------------------- fused
+// Deterministic grid reduction without a second launch: every block writes
+// its partials, then the last block to finish (atomic ticket) sums them in
+// block order.  work[0] holds the ticket (zero between launches; the last
+// block resets it), partials start at work + 1.
+
+__device__ __forceinline__ bool last_block(unsigned *ticket, unsigned nblocks)
+{
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = (atomicAdd(ticket, 1u) == nblocks - 1);
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+// Block-wide sum of n complex values per thread (vals[k]) into partial[k].
+template <int N>
+__device__ __forceinline__ void block_sum(double (&re)[N], double (&im)[N], double2 *partial, int n)
+{
+    __shared__ double red[2][8][32];  // [re/im][warp][value] (blockDim <= 256, N <= 32)
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        double a = re[k], b = im[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, off);
+            b += __shfl_down_sync(0xffffffffu, b, off);
+        }
+        if (lane == 0 && k < n) {
+            red[0][w][k] = a;
+            red[1][w][k] = b;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < n) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < nw; ++k) {
+            a += red[0][k][threadIdx.x];
+            b += red[1][k][threadIdx.x];
+        }
+        partial[threadIdx.x] = make_double2(a, b);
+    }
+}
+
+// G = op(L)^T R for nl*nr <= NLM*NRM <= 32, register accumulation over a
+// grid-stride loop of rows, fused reduction.
+template <int NLM, int NRM>
+__global__ void __launch_bounds__(256)
+    gram_small(const __grid_constant__ ColList L, const __grid_constant__ ColList R, int64_t len, int herm,
+               double2 *__restrict__ work, double2 *__restrict__ out, int ldo)
+{
+    const int nl = L.n, nr = R.n;
+    double ar[NLM * NRM], ai[NLM * NRM];
+#pragma unroll
+    for (int k = 0; k < NLM * NRM; ++k) ar[k] = ai[k] = 0.0;
+    const double sg = herm ? -1.0 : 1.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
+        double2 rv[NRM];
+#pragma unroll
+        for (int j = 0; j < NRM; ++j) rv[j] = (j < nr) ? col_elem(R, j, r) : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int i = 0; i < NLM; ++i) {
+            if (i < nl) {
+                double2 lv = col_elem(L, i, r);
+                lv.y *= sg;
+#pragma unroll
+                for (int j = 0; j < NRM; ++j) {
+                    const int k = i * NRM + j;
+                    ar[k] = fma(lv.x, rv[j].x, ar[k]);
+                    ar[k] = fma(-lv.y, rv[j].y, ar[k]);
+                    ai[k] = fma(lv.x, rv[j].y, ai[k]);
+                    ai[k] = fma(lv.y, rv[j].x, ai[k]);
+                }
+            }
+        }
+    }
+    unsigned *ticket = reinterpret_cast<unsigned *>(work);
+    double2 *part = work + 1;
+    const int nout = NLM * NRM;
+    block_sum<NLM * NRM>(ar, ai, part + (int64_t)blockIdx.x * nout, nout);
+    if (last_block(ticket, gridDim.x)) {
+        for (int o = threadIdx.x; o < nl * nr; o += blockDim.x) {
+            const int i = o / nr, j = o % nr;
+            const int k = i * NRM + j;
+            double a = 0.0, b = 0.0;
+            for (unsigned bb = 0; bb < gridDim.x; ++bb) {
+                const double2 v = __ldcg(part + (int64_t)bb * nout + k);
+                a += v.x;
+                b += v.y;
+            }
+            out[i + (int64_t)ldo * j] = make_double2(a, b);
+        }
+        if (threadIdx.x == 0) *ticket = 0u;
+    }
+}
+
+// Gram-Schmidt step of myhgramschmidt_many (harmonic_ritz_small.F90:52-59):
+//   q -= sum_i Qp_i d_i ; v -= sum_i Vp_i d_i ; c = 1/sqrt(|<q,q>|)
+// with d (m values) and the output c in device memory.
+struct GsArgs {
+    const double2 *qp[64];
+    const double2 *vp[64];
+    double2 *q, *v;
+    int m;
+};
+
+__global__ void __launch_bounds__(256)
+    gs_update(const __grid_constant__ GsArgs A, const double2 *__restrict__ d, int64_t len,
+              double2 *__restrict__ work, double2 *__restrict__ cout)
+{
+    __shared__ double2 ds[64];
+    if (threadIdx.x < A.m) ds[threadIdx.x] = d[threadIdx.x];
+    __syncthreads();
+    double nr[1] = {0.0}, ni[1] = {0.0};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
+        double2 q = A.q[r], v = A.v[r];
+        for (int i = 0; i < A.m; ++i) {
+            const double2 c = ds[i];
+            const double2 a = A.qp[i][r], b = A.vp[i][r];
+            q.x -= a.x * c.x - a.y * c.y;
+            q.y -= a.x * c.y + a.y * c.x;
+            v.x -= b.x * c.x - b.y * c.y;
+            v.y -= b.x * c.y + b.y * c.x;
+        }
+        A.q[r] = q;
+        A.v[r] = v;
+        nr[0] = fma(q.x, q.x, nr[0]);
+        nr[0] = fma(q.y, q.y, nr[0]);
+    }
+    unsigned *ticket = reinterpret_cast<unsigned *>(work);
+    double2 *part = work + 1;
+    block_sum<1>(nr, ni, part + blockIdx.x, 1);
+    if (last_block(ticket, gridDim.x)) {
+        if (threadIdx.x == 0) {
+            double a = 0.0;
+            for (unsigned bb = 0; bb < gridDim.x; ++bb) a += __ldcg(part + bb).x;
+            cout[0] = make_double2(1.0 / sqrt(fabs(a)), 0.0);
+            *ticket = 0u;
+        }
+    }
+}
+
+__global__ void gs_scale(double2 *__restrict__ q, double2 *__restrict__ v, const double2 *__restrict__ c, int64_t len)
+{
+    const double s = c[0].x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
+        const double2 a = q[r], b = v[r];
+        q[r] = make_double2(a.x * s, a.y * s);
+        v[r] = make_double2(b.x * s, b.y * s);
+    }
+}
+
 int stream_blocks(int64_t len)
 {
     return (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, 148 * 4));
@@ -332,13 +499,58 @@ int stream_blocks(int64_t len)
 
 int64_t gram_work_elems(int nl, int nr, int64_t len)
 {
-    return (int64_t)gram_blocks(nl, nr, len) * nl * nr;
+    return 1 + std::max<int64_t>((int64_t)gram_blocks(nl, nr, len) * nl * nr, (int64_t)kSmallBlocks * 32);
+}
+
+template <int A, int B>
+static cudaError_t gram_small_go(const ColList &L, const ColList &R, int64_t len, int herm, double2 *out, int ldo,
+                                 double2 *work, cudaStream_t st)
+{
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, kSmallBlocks));
+    gram_small<A, B><<<blocks, 256, 0, st>>>(L, R, len, herm, work, out, ldo);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t gs_update_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
+                             const double2 *d, int64_t len, double2 *work, double2 *cout, cudaStream_t st)
+{
+    if (m < 0 || m > 64) return cudaErrorInvalidValue;
+    GsArgs A{};
+    for (int i = 0; i < m; ++i) {
+        A.qp[i] = qp[i];
+        A.vp[i] = vp[i];
+    }
+    A.q = q;
+    A.v = v;
+    A.m = m;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, kSmallBlocks));
+    gs_update<<<blocks, 256, 0, st>>>(A, d, len, work, cout);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    gs_scale<<<blocks, 256, 0, st>>>(q, v, cout, len);
+    count_launch();
+    return cudaGetLastError();
 }
 
 cudaError_t gram_launch(const ColList &L, const ColList &R, int64_t len, int herm, double2 *out,
                         int ldo, double2 *work, cudaStream_t st)
 {
     if (L.n < 1 || L.n > 64 || R.n < 1 || R.n > 128 || len < 1) return cudaErrorInvalidValue;
+    if (R.n == 1 && L.n <= 32) {
+        if (L.n <= 1) return gram_small_go<1, 1>(L, R, len, herm, out, ldo, work, st);
+        if (L.n <= 2) return gram_small_go<2, 1>(L, R, len, herm, out, ldo, work, st);
+        if (L.n <= 4) return gram_small_go<4, 1>(L, R, len, herm, out, ldo, work, st);
+        if (L.n <= 8) return gram_small_go<8, 1>(L, R, len, herm, out, ldo, work, st);
+        if (L.n <= 16) return gram_small_go<16, 1>(L, R, len, herm, out, ldo, work, st);
+        return gram_small_go<32, 1>(L, R, len, herm, out, ldo, work, st);
+    }
+    if (L.n <= 2 && R.n <= 2) return gram_small_go<2, 2>(L, R, len, herm, out, ldo, work, st);
+    if (L.n <= 4 && R.n <= 4) return gram_small_go<4, 4>(L, R, len, herm, out, ldo, work, st);
+    if (L.n <= 8 && R.n <= 4) return gram_small_go<8, 4>(L, R, len, herm, out, ldo, work, st);
+    if (L.n <= 4 && R.n <= 8) return gram_small_go<4, 8>(L, R, len, herm, out, ldo, work, st);
+    work += 1;  // the tiled path does not use the ticket
     const int nblk = gram_blocks(L.n, R.n, len);
     int64_t chunk = (len + nblk - 1) / nblk;
     chunk = (chunk + kGramRT - 1) / kGramRT * kGramRT;
@@ -355,6 +567,7 @@ cudaError_t gram_launch(const ColList &L, const ColList &R, int64_t len, int her
     if (e != cudaSuccess) return e;
     const int nout = L.n * R.n;
     gram_reduce<<<(nout + 255) / 256, 256, 0, st>>>(work, nblk, L.n, R.n, out, ldo);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -381,6 +594,7 @@ cudaError_t axpc_launch(double2 *const *out, const double2 *const *a, const doub
         P.b[j] = b[j];
     }
     axpc_kernel<<<dim3(stream_blocks(len) / n + 1, n), 256, 0, st>>>(P, s, c_dev, len);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -391,13 +605,14 @@ cudaError_t scale_cols_launch(double2 *const *x, int n, const double2 *c_dev, in
     PtrPack P{};
     for (int j = 0; j < n; ++j) P.out[j] = x[j];
     scale_kernel<<<dim3(stream_blocks(len) / n + 1, n), 256, 0, st>>>(P, c_dev, len);
+    count_launch();
     return cudaGetLastError();
 }
 
 int64_t dotdiag_work_elems(int n, int64_t len)
 {
     (void)len;
-    return (int64_t)n * 296;
+    return 1 + (int64_t)n * 296;
 }
 
 cudaError_t dotdiag_launch(const double2 *const *a, const double2 *const *b, int n, int64_t len,
@@ -409,11 +624,14 @@ cudaError_t dotdiag_launch(const double2 *const *a, const double2 *const *b, int
         P.a[j] = a[j];
         P.b[j] = b[j];
     }
+    work += 1;
     const int nblk = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, std::max(1, 296 / n)));
     dotdiag_partial<<<dim3(nblk, n), 256, 0, st>>>(P, len, herm, work);
+    count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dotdiag_reduce<<<1, 64, 0, st>>>(work, nblk, n, out);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -421,6 +639,7 @@ cudaError_t inv_sqrt_abs_launch(const double2 *d, double2 *c, int n, cudaStream_
 {
     if (n < 1 || n > 64) return cudaErrorInvalidValue;
     inv_sqrt_abs_kernel<<<1, 64, 0, st>>>(d, c, n);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -428,6 +647,7 @@ cudaError_t build_tables_launch(int nn, int n, double charge, double delta, cons
                                 int nbd, double *t1a, double *v12, cudaStream_t st)
 {
     tables_kernel<<<148, 256, 0, st>>>(nn, n, charge, delta, tinv, nbd, t1a, v12);
+    count_launch();
     return cudaGetLastError();
 }
 

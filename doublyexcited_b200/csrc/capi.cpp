@@ -18,6 +18,8 @@ using namespace de;
 
 extern "C" {
 
+DE_API int64_t de_kernel_launches(void) { return launch_count(); }
+
 DE_API const char *de_version(void) { return "doublyexcited-b200 0.1 (sm_100a, FP64)"; }
 
 DE_API const char *de_last_error(void) { return last_error_str(); }
@@ -113,15 +115,96 @@ int de_problem::ensure_work(int64_t elems)
     d_work = nullptr;
     work_elems = 0;
     DE_CUDA(cudaMalloc(&d_work, elems * sizeof(double2)));
+    DE_CUDA(cudaMemset(d_work, 0, sizeof(double2)));  // reduction ticket
     work_elems = elems;
+    return DE_OK;
+}
+
+void *de_problem::cache_get(size_t bytes)
+{
+    Blk *best = nullptr;
+    for (auto &b : cache)
+        if (!b.used && b.bytes >= bytes && b.bytes <= 2 * bytes + (1 << 20) && (!best || b.bytes < best->bytes)) best = &b;
+    if (best) {
+        best->used = true;
+        return best->p;
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        // release idle blocks and retry once
+        for (auto it = cache.begin(); it != cache.end();) {
+            if (!it->used) {
+                cudaFree(it->p);
+                it = cache.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    }
+    cache.push_back(Blk{p, bytes, true});
+    return p;
+}
+
+void de_problem::cache_put(void *p)
+{
+    for (auto &b : cache)
+        if (b.p == p) b.used = false;
+}
+
+cudaEvent_t de_problem::take_event()
+{
+    if (!ev_free.empty()) {
+        cudaEvent_t e = ev_free.back();
+        ev_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+int de_problem::harvest()
+{
+    for (auto &r : ev_pending) {
+        DE_CUDA(cudaEventSynchronize(r.e[2]));
+        float a = 0.f, b = 0.f;
+        DE_CUDA(cudaEventElapsedTime(&a, r.e[0], r.e[1]));
+        DE_CUDA(cudaEventElapsedTime(&b, r.e[1], r.e[2]));
+        prof_ms[0] += a;
+        prof_ms[1] += b;
+        prof_calls += 1;
+        prof_vectors += r.nvec;
+        for (auto ev : r.e) ev_free.push_back(ev);
+    }
+    ev_pending.clear();
     return DE_OK;
 }
 
 int de_problem::matblock(const double2 *x, double2 *y, int nvec)
 {
-    cudaError_t e = (p.nelec == 2) ? hammult_launch(ham, x, y, nvec, dim, stream)
-                                   : hammult1_launch(ham, d_t1a, x, y, nvec, dim, stream);
-    if (e != cudaSuccess) return cuda_error(e, "hammult");
+    if (p.nelec != 2) {
+        cudaError_t e = hammult1_launch(ham, d_t1a, x, y, nvec, dim, stream);
+        if (e != cudaSuccess) return cuda_error(e, "hammult1");
+        return DE_OK;
+    }
+    Rec r{{nullptr, nullptr, nullptr}, nvec};
+    if (prof) {
+        for (auto &ev : r.e)
+            if (!(ev = take_event())) return set_error(DE_E_CUDA, "cudaEventCreate failed");
+        DE_CUDA(cudaEventRecord(r.e[0], stream));
+    }
+    cudaError_t e = hammult_pass_launch(ham, x, y, nvec, dim, 0, stream);
+    if (e != cudaSuccess) return cuda_error(e, "hammult pass A");
+    if (prof) DE_CUDA(cudaEventRecord(r.e[1], stream));
+    e = hammult_pass_launch(ham, x, y, nvec, dim, 1, stream);
+    if (e != cudaSuccess) return cuda_error(e, "hammult pass B");
+    if (prof) {
+        DE_CUDA(cudaEventRecord(r.e[2], stream));
+        ev_pending.push_back(r);
+        if (ev_pending.size() > 4096) DE_TRY(harvest());
+    }
     return DE_OK;
 }
 
@@ -170,6 +253,8 @@ DE_API int de_problem_create(const de_params *pin, de_problem **out)
     hd.s2im = s2.imag();
     hd.vsre = vs.real();
     hd.vsim = vs.imag();
+    hd.sre = scale.real();
+    hd.sim = scale.imag();
 
     auto tinv = cached_tinv(nbig_alloc, nbig_solve, p.nsmall, delta);
     const int nbd = 2 * nbig_alloc + 1;
@@ -206,6 +291,10 @@ DE_API int de_problem_destroy(de_problem *h)
     cudaFree(h->d_work);
     cudaFreeHost(h->h_small);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    for (auto &r : h->ev_pending)
+        for (auto ev : r.e) cudaEventDestroy(ev);
+    for (auto ev : h->ev_free) cudaEventDestroy(ev);
+    for (auto &b : h->cache) cudaFree(b.p);
     delete h;
     return DE_OK;
 }
@@ -223,6 +312,27 @@ DE_API int de_set_stream(de_problem *h, void *s)
 {
     if (!h) return set_error(DE_E_INVALID, "null handle");
     h->stream = s ? (cudaStream_t)s : cudaStreamLegacy;
+    return DE_OK;
+}
+
+DE_API int de_set_profiling(de_problem *h, int on)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    h->prof = on != 0;
+    return DE_OK;
+}
+
+DE_API int de_profile_read(de_problem *h, double *pass_a_ms, double *pass_b_ms, int64_t *calls, int64_t *vectors)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    cudaSetDevice(h->p.device);
+    DE_TRY(h->harvest());
+    if (pass_a_ms) *pass_a_ms = h->prof_ms[0];
+    if (pass_b_ms) *pass_b_ms = h->prof_ms[1];
+    if (calls) *calls = h->prof_calls;
+    if (vectors) *vectors = h->prof_vectors;
+    h->prof_ms[0] = h->prof_ms[1] = 0.0;
+    h->prof_calls = h->prof_vectors = 0;
     return DE_OK;
 }
 

@@ -86,6 +86,28 @@ struct de_problem {
     int64_t work_elems = 0;
     double2 *h_small = nullptr;   // pinned mirror of d_small
     std::mutex mu;
+    // matvec device-time accounting (de_set_profiling)
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_free;
+    struct Rec {
+        cudaEvent_t e[3];
+        int nvec;
+    };
+    std::vector<Rec> ev_pending;
+    double prof_ms[2] = {0.0, 0.0};
+    int64_t prof_calls = 0, prof_vectors = 0;
+    int harvest();
+    cudaEvent_t take_event();
+
+    // device workspace cache reused across solves (best fit)
+    struct Blk {
+        void *p;
+        size_t bytes;
+        bool used;
+    };
+    std::vector<Blk> cache;
+    void *cache_get(size_t bytes);
+    void cache_put(void *p);
 
     int ensure_stage(int64_t elems);
     int ensure_work(int64_t elems);

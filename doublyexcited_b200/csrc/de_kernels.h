@@ -8,6 +8,10 @@
 
 namespace de {
 
+// Process-wide count of kernels launched by this library.
+void count_launch(int n = 1);
+int64_t launch_count();
+
 constexpr int kMaxNN = 27;      // N <= 13 (the reference ran N = 5..15)
 constexpr int kMaxCols = 128;   // columns per block-op operand list
 
@@ -19,6 +23,7 @@ struct HamDev {
     double t[kMaxNN];       // T_real(0,d) = KEMATRIX first column, d = 0..NN-1
     double s2re, s2im;      // 1/SCALE^2 (initmod.F90:208)
     double vsre, vsim;      // 1/SCALE (initmod.F90:224)
+    double sre, sim;        // SCALE = exp(i theta) (initmod.F90:48)
     const double *t1a;      // [M]  A*TINV(r_p), A = -Z/delta^3 (hammod.F90:576-577)
     const double *v12;      // [(2NN-1)^3] TINV(r_q - r_p)/delta^3 (hammod.F90:578)
 };
@@ -28,6 +33,11 @@ struct HamDev {
 // electron-1 axes (contiguous cubes, Y += ...).  Deterministic (no atomics).
 cudaError_t hammult_launch(const HamDev &h, const double2 *x, double2 *y, int nvec,
                            int64_t vstride, cudaStream_t st);
+
+// One pass of the above: pass 0 = electron-2 + potential (writes Y), pass 1 =
+// electron-1 (Y += ...).
+cudaError_t hammult_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec,
+                                int64_t vstride, int pass, cudaStream_t st);
 
 // One-electron H (NELEC=1): KEMULT1 + V (hammod.F90:71-134).
 cudaError_t hammult1_launch(const HamDev &h, const double *vfull, const double2 *x, double2 *y,
@@ -70,6 +80,12 @@ cudaError_t axpc_launch(double2 *const *out, const double2 *const *a, const doub
 int64_t dotdiag_work_elems(int n, int64_t len);
 cudaError_t dotdiag_launch(const double2 *const *a, const double2 *const *b, int n, int64_t len,
                            int herm, double2 *out, double2 *work, cudaStream_t st);
+
+// Gram-Schmidt step of the inner solve: q -= sum_i qp_i d_i, v -= sum_i
+// vp_i d_i (d: m values in DEVICE memory), then q, v *= 1/sqrt(|<q,q>|); the
+// factor is also left in cout[0].  work as for gram (ticket at work[0]).
+cudaError_t gs_update_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
+                             const double2 *d, int64_t len, double2 *work, double2 *cout, cudaStream_t st);
 
 // x_j *= c_j (c from DEVICE, complex), in place.
 cudaError_t scale_cols_launch(double2 *const *x, int n, const double2 *c_dev, int64_t len,

@@ -61,7 +61,7 @@ struct Solver {
 
     ~Solver()
     {
-        for (auto p : allocs) cudaFree(p);
+        for (auto p : allocs) h->cache_put(p);
         if (hbuf) cudaFreeHost(hbuf);
     }
 
@@ -69,8 +69,8 @@ struct Solver {
 
     int alloc(double2 **p, int64_t elems)
     {
-        cudaError_t e = cudaMalloc(p, elems * sizeof(double2));
-        if (e != cudaSuccess) return cuda_error(e, "cudaMalloc (GPLMR workspace)");
+        *p = (double2 *)h->cache_get((size_t)elems * sizeof(double2));
+        if (!*p) return set_error(DE_E_NOMEM, "GPLMR workspace: cannot allocate %lld bytes", (long long)(elems * 16));
         allocs.push_back(*p);
         return DE_OK;
     }
@@ -282,19 +282,11 @@ struct Solver {
     // pairs of (LQ, LV).
     int hgram(int m, double2 *q, double2 *v)
     {
+        std::vector<const double2 *> qp = cl(LQ, m), vp = cl(LV, m);
         for (int pass = 0; pass < 2; ++pass) {
-            if (m > 0) {
-                DE_TRY(gram_dev(cols(LQ, m, D), cols(q, 1, D), dT, m));
-                DE_TRY(update(cl(LQ, m), {q}, dT, m, -1.0, 1.0));
-                DE_TRY(update(cl(LV, m), {v}, dT, m, -1.0, 1.0));
-            }
-            const double2 *qa[1] = {q};
-            cudaError_t e = dotdiag_launch(qa, qa, 1, D, 1, dR, h->d_work, st);
-            if (e != cudaSuccess) return cuda_error(e, "dotdiag");
-            if ((e = inv_sqrt_abs_launch(dR, dR + 1, 1, st)) != cudaSuccess) return cuda_error(e, "inv_sqrt");
-            double2 *qv[2] = {q, v};
-            if ((e = scale_cols_launch(qv, 1, dR + 1, D, st)) != cudaSuccess) return cuda_error(e, "scale");
-            if ((e = scale_cols_launch(qv + 1, 1, dR + 1, D, st)) != cudaSuccess) return cuda_error(e, "scale");
+            if (m > 0) DE_TRY(gram_dev(cols(LQ, m, D), cols(q, 1, D), dT, m));
+            cudaError_t e = gs_update_launch(qp.data(), vp.data(), m, q, v, dT, D, h->d_work, dR, st);
+            if (e != cudaSuccess) return cuda_error(e, "gs_update");
         }
         return DE_OK;
     }

@@ -109,6 +109,8 @@ typedef struct de_problem de_problem;
 DE_API const char *de_strerror(int status);
 DE_API const char *de_last_error(void);
 DE_API const char *de_version(void);
+/* Number of CUDA kernels this library has launched in the process. */
+DE_API int64_t de_kernel_launches(void);
 
 /* ---- parameters and set-up ------------------------------------------- */
 
@@ -129,6 +131,16 @@ DE_API int de_problem_dims(const de_problem *h, int *nn, int64_t *m, int64_t *di
  * CUDA legacy default stream (as in the CUDA runtime); a new handle uses a
  * private non-blocking stream until this is called. */
 DE_API int de_set_stream(de_problem *h, void *cuda_stream);
+
+/* Device-time accounting of the matvec kernels: CUDA events recorded on the
+ * handle's stream around the two passes of every MATBLOCK (pass A: electron-2
+ * contraction + potential; pass B: electron-1 contraction).  Off by default.
+ * The reference times phases with MPI_WTIME (gplmr.F90:42-57). */
+DE_API int de_set_profiling(de_problem *h, int on);
+/* Device milliseconds of pass A and pass B, MATBLOCK calls and vectors
+ * multiplied since the last read (waits for the recorded events); resets. */
+DE_API int de_profile_read(de_problem *h, double *pass_a_ms, double *pass_b_ms, int64_t *calls,
+                           int64_t *vectors);
 
 /* ---- operator: HAMMULT / MATBLOCK / MYMATMUL ------------------------- */
 

@@ -134,6 +134,7 @@ FIXTURES = {
     "gplmr_n3_nev4": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 4, False, 12, 1e-10))),
     "gplmr_n3_nev4_compat": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 4, True, 12, 1e-10))),
     "gplmr_n5_nev1": (True, lambda: ("json", gplmr_fixture(5, 0.2, complex(-0.7131541429, 0), 1, False, 60, 1e-9))),
+    "gplmr_n6_nev1": (True, lambda: ("json", gplmr_fixture(6, 0.2, complex(-0.7131541429, 0), 1, False, 80, 1e-8))),
 }
 
 
@@ -152,6 +153,9 @@ def main():
         if kind == "json":
             if name.startswith("gplmr_n5"):
                 data["reference_log"] = {"e": list(RESONANCE_LOG["n5"]), "source": "CSCALE-WORK/Outs/Out.S.N5:147"}
+            if name.startswith("gplmr_n6"):
+                data["reference_log"] = {"e": list(RESONANCE_LOG["n6_basic"]),
+                                         "source": "CSCALE-WORK/Outs/Out.S.D2d0.T0.2d0.N6.petsc:97"}
             with open(os.path.join(HERE, name + ".json"), "w") as f:
                 json.dump(data, f, indent=1)
         else:
