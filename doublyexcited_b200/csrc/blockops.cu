@@ -11,10 +11,12 @@
 //
 // Every kernel here streams its vectors once; they are HBM-bound except the
 // 64 x 64 projection Gram, which is FP64-FMA bound (8 flops per complex MAC).
+#include "de_internal.h"
 #include "de_kernels.h"
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 
 namespace de {
 
@@ -652,3 +654,84 @@ cudaError_t build_tables_launch(int nn, int n, double charge, double delta, cons
 }
 
 }  // namespace de
+
+// ---------------------------------------------------------------- no-alloc
+// Allocation-free variant of the device dot products, for callers that must
+// not allocate device memory: code recording work into a CUDA graph or
+// running under a pre-reserved memory budget, where a cudaMalloc would break
+// the capture or exceed the reservation.  Its reduction scratch (ticket plus
+// one partial per block and output of the fused small Gram) is a file-scope
+// device array of 1 + 296*32 complex values (151,568 bytes) that every GPU
+// loading this library holds until the process exits.
+
+namespace de {
+
+static __device__ __align__(256) double2 g_dots_scratch[1 + kSmallBlocks * 32];
+
+namespace {
+std::mutex g_scratch_mu;
+double2 *g_scratch_ptr[64] = {};
+}  // namespace
+
+}  // namespace de
+
+extern "C" DE_API int de_dots_noalloc_d(const de_complex *bras_d, const de_complex *kets_d, int64_t size, int nbra,
+                                        int nket, de_complex *out_d, int hermitian, void *cuda_stream)
+{
+    using namespace de;
+    if (!bras_d || !kets_d || !out_d) return set_error(DE_E_INVALID, "de_dots_noalloc_d: null pointer");
+    if (size < 1 || nbra < 1 || nket < 1) return set_error(DE_E_INVALID, "de_dots_noalloc_d: empty dot");
+    const bool shape_ok = (nket == 1 && nbra <= 32) || (nbra <= 4 && nket <= 4) || (nbra <= 8 && nket <= 4) ||
+                          (nbra <= 4 && nket <= 8);
+    if (!shape_ok)
+        return set_error(DE_E_INVALID,
+                         "de_dots_noalloc_d: %d x %d outputs exceed the allocation-free maximum "
+                         "(nket == 1 with nbra <= 32, or nbra*nket <= 32 with both <= 8 and one <= 4)",
+                         nbra, nket);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+    if (dev < 0 || dev >= 64) return set_error(DE_E_INVALID, "de_dots_noalloc_d: device ordinal %d", dev);
+    double2 *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        if (!g_scratch_ptr[dev]) {
+            // First call on this device: host code needs the device address of
+            // the array (its host-side symbol is only a stand-in).
+            e = cudaGetSymbolAddress((void **)&g_scratch_ptr[dev], g_dots_scratch);
+            if (e != cudaSuccess) {
+                g_scratch_ptr[dev] = nullptr;
+                return cuda_error(e, "cudaGetSymbolAddress(dots scratch)");
+            }
+        }
+        scratch = g_scratch_ptr[dev];
+    }
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    // the reduction ticket must start at zero whatever the previous call left
+    e = cudaMemsetAsync(scratch, 0, sizeof(double2), st);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(dots scratch)");
+    ColList L{}, R{};
+    L.n = nbra;
+    R.n = nket;
+    for (int i = 0; i < nbra; ++i) L.a[i] = (const double2 *)bras_d + (int64_t)i * size;
+    for (int j = 0; j < nket; ++j) R.a[j] = (const double2 *)kets_d + (int64_t)j * size;
+    double2 *out = (double2 *)out_d;
+    const int herm = hermitian ? 1 : 0;
+    if (nket == 1) {
+        if (nbra <= 1) e = gram_small_go<1, 1>(L, R, size, herm, out, nbra, scratch, st);
+        else if (nbra <= 2) e = gram_small_go<2, 1>(L, R, size, herm, out, nbra, scratch, st);
+        else if (nbra <= 4) e = gram_small_go<4, 1>(L, R, size, herm, out, nbra, scratch, st);
+        else if (nbra <= 8) e = gram_small_go<8, 1>(L, R, size, herm, out, nbra, scratch, st);
+        else if (nbra <= 16) e = gram_small_go<16, 1>(L, R, size, herm, out, nbra, scratch, st);
+        else e = gram_small_go<32, 1>(L, R, size, herm, out, nbra, scratch, st);
+    } else if (nbra <= 4 && nket <= 4) {
+        e = gram_small_go<4, 4>(L, R, size, herm, out, nbra, scratch, st);
+    } else if (nket <= 4) {
+        e = gram_small_go<8, 4>(L, R, size, herm, out, nbra, scratch, st);
+    } else {
+        e = gram_small_go<4, 8>(L, R, size, herm, out, nbra, scratch, st);
+    }
+    if (e != cudaSuccess) return cuda_error(e, "de_dots_noalloc_d launch");
+    return DE_OK;
+}
+

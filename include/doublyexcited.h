@@ -166,6 +166,23 @@ DE_API int de_dots(de_problem *h, const de_complex *bras, const de_complex *kets
 DE_API int de_dots_d(de_problem *h, const de_complex *bras_d, const de_complex *kets_d,
                      int64_t size, int nbra, int nket, de_complex *out_host, int hermitian);
 
+/* Allocation-free device dot products.  No counterpart in the reference.
+ * For callers that cannot allocate device memory: code recording work into a
+ * CUDA graph, or running inside a pre-reserved memory budget, where a
+ * cudaMalloc would break the capture or the reservation.  Same results as
+ * de_dots_d (hermitian=1: conj(BRA).KET; 0: the c-product), written to DEVICE
+ * memory out_d (nbra x nket column-major) asynchronously on cuda_stream (NULL:
+ * legacy default stream).  Needs no handle and allocates nothing: the
+ * reduction scratch is a static device array of 151,568 bytes that every GPU
+ * loading the library holds until exit.  Shapes: nket == 1 with nbra <= 32,
+ * or nbra, nket <= 8 with one of them <= 4 (at most 32 outputs); larger shapes
+ * return DE_E_INVALID.  The first call on each device looks up the array's
+ * device address (make it before any stream capture).  All calls share the
+ * array: calls that overlap on the GPU (other streams, other host threads)
+ * race and must be serialised by the caller. */
+DE_API int de_dots_noalloc_d(const de_complex *bras_d, const de_complex *kets_d, int64_t size, int nbra,
+                             int nket, de_complex *out_d, int hermitian, void *cuda_stream);
+
 /* EXPECTS(j) = <psi_j|H|psi_j>/<psi_j|psi_j> (Hermitian; c-product when
  * cshiftopt).  GET_EXPECTS hammod.F90:1261-1301. */
 DE_API int de_get_expects(de_problem *h, const de_complex *psi, int nvec, int cshiftopt,
