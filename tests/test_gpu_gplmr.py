@@ -37,13 +37,16 @@ def test_gplmr_n3_nev1_converged(de, oracle):
 
 
 def test_gplmr_n3_nev4_tracks_oracle(de, oracle):
-    """NEV=4 for 12 iterations: the Ritz values agree with the oracle's."""
+    """NEV=4: the four Ritz values after 6 iterations agree with the oracle's.
+    (Later iterations of this unconverged block are chaotic: the oracle
+    restarted from a start vector perturbed by 1e-14 differs from itself by
+    1e-7 at iteration 9 and 1e-4 at iteration 12, so they are no parity test.)"""
     g = load_json("gplmr_n3_nev4.json")
-    r = _run(de, oracle, g)
-    assert r.iterations == g["iterations"]
-    e = np.array([complex(*z) for z in g["e"]])
-    assert np.max(np.abs(np.sort_complex(r.e) - np.sort_complex(e))) < 1e-8
-    assert r.matvecs_reference == g["matvecs_reference"]
+    k = 6
+    r = _run(de, oracle, g, maxit=k)
+    assert r.iterations == k
+    e = np.array([complex(*z) for z in g["history"][k - 1]["e"]])
+    assert np.max(np.abs(np.sort_complex(r.e) - np.sort_complex(e))) < 1e-10
 
 
 def test_gplmr_first_column_only_mode_stops_like_the_reference(de, oracle):
