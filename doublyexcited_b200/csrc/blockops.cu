@@ -136,7 +136,7 @@ __global__ void gram_reduce(const double2 *__restrict__ work, int nblk, int nl, 
 int gram_blocks(int nl, int nr, int64_t len)
 {
     const int64_t tiles = (len + kGramRT - 1) / kGramRT;
-    const int64_t cap = (int64_t)nl * nr > 1024 ? 296 : 592;
+    const int64_t cap = (int64_t)nl * nr > 1024 ? 296 : 148 * 8;
     return (int)std::max<int64_t>(1, std::min(tiles, cap));
 }
 
@@ -492,6 +492,205 @@ __global__ void gs_scale(double2 *__restrict__ q, double2 *__restrict__ v, const
     }
 }
 
+// Second pass of the fused two-pass Gram-Schmidt: with the pass-1
+// coefficients d (device), q -= Qp d and v -= Vp d, then the pass-2
+// coefficients <Qp_i, q> (i < m) are reduced into dout (m values).
+template <int MM>
+__global__ void __launch_bounds__(256)
+    gs_pass1(const __grid_constant__ GsArgs A, const double2 *__restrict__ d, int64_t len,
+             double2 *__restrict__ work, double2 *__restrict__ dout)
+{
+    __shared__ double2 ds[64];
+    if (threadIdx.x < A.m) ds[threadIdx.x] = d[threadIdx.x];
+    __syncthreads();
+    double ar[MM + 1], ai[MM + 1];
+#pragma unroll
+    for (int i = 0; i <= MM; ++i) ar[i] = ai[i] = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
+        double2 q = A.q[r], v = A.v[r];
+        double2 a[MM];
+#pragma unroll
+        for (int i = 0; i < MM; ++i) {
+            if (i < A.m) {
+                const double2 c = ds[i];
+                a[i] = A.qp[i][r];
+                const double2 b = A.vp[i][r];
+                q.x -= a[i].x * c.x - a[i].y * c.y;
+                q.y -= a[i].x * c.y + a[i].y * c.x;
+                v.x -= b.x * c.x - b.y * c.y;
+                v.y -= b.x * c.y + b.y * c.x;
+            }
+        }
+        A.q[r] = q;
+        A.v[r] = v;
+#pragma unroll
+        for (int i = 0; i < MM; ++i) {
+            if (i < A.m) {  // conj(a_i) q
+                ar[i] = fma(a[i].x, q.x, ar[i]);
+                ar[i] = fma(a[i].y, q.y, ar[i]);
+                ai[i] = fma(a[i].x, q.y, ai[i]);
+                ai[i] = fma(-a[i].y, q.x, ai[i]);
+            }
+        }
+        ar[MM] = fma(q.x, q.x, ar[MM]);
+        ar[MM] = fma(q.y, q.y, ar[MM]);
+    }
+    unsigned *ticket = reinterpret_cast<unsigned *>(work);
+    double2 *part = work + 1;
+    block_sum<MM + 1>(ar, ai, part + (int64_t)blockIdx.x * (MM + 1), MM + 1);
+    if (last_block(ticket, gridDim.x)) {
+        for (int o = threadIdx.x; o <= MM; o += blockDim.x) {
+            if (o < A.m || o == MM) {
+                double x = 0.0, y = 0.0;
+                for (unsigned bb = 0; bb < gridDim.x; ++bb) {
+                    const double2 w = __ldcg(part + (int64_t)bb * (MM + 1) + o);
+                    x += w.x;
+                    y += w.y;
+                }
+                dout[o == MM ? 64 : o] = make_double2(x, y);  // |u|^2 goes to dout[64]
+            }
+        }
+        if (threadIdx.x == 0) *ticket = 0u;
+    }
+}
+
+// Second pass with the normalisation folded in: q <- (q - Qp d2)/|w|,
+// v <- (v - Vp d2)/|w| where |w|^2 = |u|^2 - |d2|^2 (Pythagoras; u is the
+// pass-1 vector, whose component in span(Qp) is already at rounding level,
+// so the subtraction loses nothing).
+__global__ void __launch_bounds__(256)
+    gs_pass2(const __grid_constant__ GsArgs A, const double2 *__restrict__ d2, int64_t len, double2 *cout)
+{
+    __shared__ double2 ds[64];
+    __shared__ double scale;
+    if (threadIdx.x < A.m) ds[threadIdx.x] = d2[threadIdx.x];
+    if (threadIdx.x == 0) {
+        double w2 = d2[64].x;
+        for (int i = 0; i < A.m; ++i) w2 -= d2[i].x * d2[i].x + d2[i].y * d2[i].y;
+        scale = 1.0 / sqrt(fabs(w2));
+        if (blockIdx.x == 0) cout[0] = make_double2(scale, 0.0);
+    }
+    __syncthreads();
+    const double sc = scale;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
+        double2 q = A.q[r], v = A.v[r];
+        for (int i = 0; i < A.m; ++i) {
+            const double2 c = ds[i];
+            const double2 a = A.qp[i][r], b = A.vp[i][r];
+            q.x -= a.x * c.x - a.y * c.y;
+            q.y -= a.x * c.y + a.y * c.x;
+            v.x -= b.x * c.x - b.y * c.y;
+            v.y -= b.x * c.y + b.y * c.x;
+        }
+        A.q[r] = make_double2(q.x * sc, q.y * sc);
+        A.v[r] = make_double2(v.x * sc, v.y * sc);
+    }
+}
+
+// ---------------------------------------------------------------- k x k
+// Dense k x k work kept on the device (k <= 16) so the solver does not stop
+// for the host: one thread each, column-major, flags reported through `flag`.
+
+// flag[0] accumulates every raised bit, flag[1] keeps the first one, so the
+// error reported is the one the reference would have stopped at.
+__device__ __forceinline__ void raise_flag(int *flag, int bit)
+{
+    atomicOr(flag, bit);
+    atomicCAS(flag + 1, 0, bit);
+}
+
+// Upper Cholesky R of the Hermitian G (upper triangle read, as zpotrf 'U')
+// and R^{-1}.  flag |= 1 on breakdown, 2 when G is all zero.
+__global__ void small_cholinv(const double2 *__restrict__ G, int k, double2 *__restrict__ Rinv, int *flag)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double2 R[16 * 16];
+    double rsum = 0.0;
+    for (int j = 0; j < k; ++j)
+        for (int i = 0; i < k; ++i) rsum += hypot(G[i + k * j].x, G[i + k * j].y);
+    if (rsum == 0.0) {
+        raise_flag(flag, 2);
+        return;
+    }
+    for (int j = 0; j < k; ++j) {
+        double dj = G[j + k * j].x;
+        for (int i = 0; i < j; ++i) dj -= R[i + k * j].x * R[i + k * j].x + R[i + k * j].y * R[i + k * j].y;
+        if (!(dj > 0.0)) {
+            raise_flag(flag, 1);
+            return;
+        }
+        const double rjj = sqrt(dj);
+        R[j + k * j] = make_double2(rjj, 0.0);
+        for (int l = j + 1; l < k; ++l) {
+            double2 s = G[j + k * l];
+            for (int i = 0; i < j; ++i) {  // s -= conj(R(i,j)) R(i,l)
+                const double2 a = R[i + k * j], b = R[i + k * l];
+                s.x -= a.x * b.x + a.y * b.y;
+                s.y -= a.x * b.y - a.y * b.x;
+            }
+            R[j + k * l] = make_double2(s.x / rjj, s.y / rjj);
+        }
+        for (int l = 0; l < j; ++l) R[j + k * l] = make_double2(0.0, 0.0);
+    }
+    for (int j = 0; j < k; ++j)  // R x = e_j by back substitution
+        for (int i = j; i >= 0; --i) {
+            double2 s = make_double2(i == j ? 1.0 : 0.0, 0.0);
+            for (int l = i + 1; l <= j; ++l) {
+                const double2 a = R[i + k * l], b = Rinv[l + k * j];
+                s.x -= a.x * b.x - a.y * b.y;
+                s.y -= a.x * b.y + a.y * b.x;
+            }
+            const double rii = R[i + k * i].x;
+            Rinv[i + k * j] = make_double2(s.x / rii, s.y / rii);
+        }
+    for (int j = 0; j < k; ++j)
+        for (int i = j + 1; i < k; ++i) Rinv[i + k * j] = make_double2(0.0, 0.0);
+}
+
+// 1 x 1 case of gen_cmatsub flag 2 (hr_eigen.f90:223-291): g > 0 real.
+__global__ void small_hsqrt1(const double2 *__restrict__ g, double2 *__restrict__ ginvh, double2 *__restrict__ gsq,
+                             int *flag)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double s = hypot(g[0].x, g[0].y);  // the singular value of the 1 x 1 matrix
+    if (!(s > 0.0)) {
+        raise_flag(flag, 8);
+        return;
+    }
+    ginvh[0] = make_double2(sqrt(1.0 / s), 0.0);
+    gsq[0] = make_double2(sqrt(s), 0.0);
+}
+
+// harm_orthog_oneblock's self-check (harmonic_ritz_small.F90:221-242):
+// flag |= 4 when any |T - I| > 1e-10.
+__global__ void small_ortho_check(const double2 *__restrict__ t, int k, int *flag)
+{
+    const int o = threadIdx.x;
+    if (o < k * k) {
+        const int i = o % k, j = o / k;
+        const double re = t[o].x - (i == j ? 1.0 : 0.0);
+        if (!(hypot(re, t[o].y) <= 1e-10)) raise_flag(flag, 4);
+    }
+}
+
+// C (m x n) = A (m x k) B (k x n), all small, column-major.
+__global__ void small_gemm(const double2 *__restrict__ A, const double2 *__restrict__ B, double2 *__restrict__ C,
+                           int m, int k, int n)
+{
+    const int o = threadIdx.x + blockIdx.x * blockDim.x;
+    if (o >= m * n) return;
+    const int i = o % m, j = o / m;
+    double2 s = make_double2(0.0, 0.0);
+    for (int l = 0; l < k; ++l) {
+        const double2 a = A[i + (int64_t)m * l], b = B[l + (int64_t)k * j];
+        s.x += a.x * b.x - a.y * b.y;
+        s.y += a.x * b.y + a.y * b.x;
+    }
+    C[o] = s;
+}
+
 int stream_blocks(int64_t len)
 {
     return (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, 148 * 4));
@@ -633,6 +832,76 @@ cudaError_t dotdiag_launch(const double2 *const *a, const double2 *const *b, int
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     dotdiag_reduce<<<1, 64, 0, st>>>(work, nblk, n, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t gs_pass1_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
+                            const double2 *d, int64_t len, double2 *work, double2 *dout, cudaStream_t st)
+{
+    if (m < 1 || m > 16) return cudaErrorInvalidValue;
+    GsArgs A{};
+    for (int i = 0; i < m; ++i) {
+        A.qp[i] = qp[i];
+        A.vp[i] = vp[i];
+    }
+    A.q = q;
+    A.v = v;
+    A.m = m;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, kSmallBlocks));
+    if (m <= 1) gs_pass1<1><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+    else if (m <= 2) gs_pass1<2><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+    else if (m <= 4) gs_pass1<4><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+    else if (m <= 8) gs_pass1<8><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+    else gs_pass1<16><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t gs_pass2_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
+                            const double2 *d2, int64_t len, double2 *cout, cudaStream_t st)
+{
+    if (m < 1 || m > 64) return cudaErrorInvalidValue;
+    GsArgs A{};
+    for (int i = 0; i < m; ++i) {
+        A.qp[i] = qp[i];
+        A.vp[i] = vp[i];
+    }
+    A.q = q;
+    A.v = v;
+    A.m = m;
+    gs_pass2<<<stream_blocks(len) * 2, 256, 0, st>>>(A, d2, len, cout);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t small_cholinv_launch(const double2 *g, int k, double2 *rinv, int *flag, cudaStream_t st)
+{
+    if (k < 1 || k > 16) return cudaErrorInvalidValue;
+    small_cholinv<<<1, 32, 0, st>>>(g, k, rinv, flag);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t small_hsqrt1_launch(const double2 *g, double2 *ginvh, double2 *gsq, int *flag, cudaStream_t st)
+{
+    small_hsqrt1<<<1, 32, 0, st>>>(g, ginvh, gsq, flag);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t small_ortho_check_launch(const double2 *t, int k, int *flag, cudaStream_t st)
+{
+    if (k < 1 || k > 16) return cudaErrorInvalidValue;
+    small_ortho_check<<<1, 256, 0, st>>>(t, k, flag);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t small_gemm_launch(const double2 *a, const double2 *b, double2 *c, int m, int k, int n, cudaStream_t st)
+{
+    if (m * n < 1) return cudaErrorInvalidValue;
+    small_gemm<<<(m * n + 127) / 128, 128, 0, st>>>(a, b, c, m, k, n);
     count_launch();
     return cudaGetLastError();
 }

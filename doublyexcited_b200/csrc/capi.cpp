@@ -182,7 +182,7 @@ int de_problem::harvest()
     return DE_OK;
 }
 
-int de_problem::matblock(const double2 *x, double2 *y, int nvec)
+int de_problem::matblock(const double2 *x, double2 *y, int nvec, double2 shift)
 {
     if (p.nelec != 2) {
         cudaError_t e = hammult1_launch(ham, d_t1a, x, y, nvec, dim, stream);
@@ -195,7 +195,7 @@ int de_problem::matblock(const double2 *x, double2 *y, int nvec)
             if (!(ev = take_event())) return set_error(DE_E_CUDA, "cudaEventCreate failed");
         DE_CUDA(cudaEventRecord(r.e[0], stream));
     }
-    cudaError_t e = hammult_pass_launch(ham, x, y, nvec, dim, 0, stream);
+    cudaError_t e = hammult_pass_launch(ham, x, y, nvec, dim, 0, stream, shift);
     if (e != cudaSuccess) return cuda_error(e, "hammult pass A");
     if (prof) DE_CUDA(cudaEventRecord(r.e[1], stream));
     e = hammult_pass_launch(ham, x, y, nvec, dim, 1, stream);

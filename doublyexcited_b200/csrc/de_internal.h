@@ -54,10 +54,6 @@ std::vector<double> kematrix(int nn, double delta);
 void jacobi_eigen(int n, std::vector<double> a, std::vector<double> &e, std::vector<double> &v);
 
 // ---- small dense helpers (host) -----------------------------------------
-// Upper Cholesky R of a Hermitian k x k (column-major); returns LAPACK info.
-int zpotrf_upper(int k, std::vector<cplx> &a);
-// Inverse of an upper-triangular k x k matrix (column-major).
-std::vector<cplx> upper_inverse(int k, const std::vector<cplx> &r);
 // gen_cmatsub flag=2 (hr_eigen.f90:223-291): returns DE status.
 int herm_sqrt_pair(int k, const std::vector<cplx> &g, std::vector<cplx> &ginvsqrt,
                    std::vector<cplx> &gsqrt);
@@ -111,5 +107,6 @@ struct de_problem {
 
     int ensure_stage(int64_t elems);
     int ensure_work(int64_t elems);
-    int matblock(const double2 *x, double2 *y, int nvec);  // device pointers
+    // device pointers; y = (H + shift) x
+    int matblock(const double2 *x, double2 *y, int nvec, double2 shift = double2{0.0, 0.0});
 };

@@ -31,13 +31,14 @@ struct HamDev {
 // Y(:,:,v) = H X(:,:,v) for v < nvec; vectors are vstride elements apart.
 // Two passes: electron-2 axes + potential (strided cubes, writes Y), then
 // electron-1 axes (contiguous cubes, Y += ...).  Deterministic (no atomics).
+// shift: y = (H + shift) x, fused into the potential term of pass A.
 cudaError_t hammult_launch(const HamDev &h, const double2 *x, double2 *y, int nvec,
-                           int64_t vstride, cudaStream_t st);
+                           int64_t vstride, cudaStream_t st, double2 shift = double2{0.0, 0.0});
 
 // One pass of the above: pass 0 = electron-2 + potential (writes Y), pass 1 =
 // electron-1 (Y += ...).
 cudaError_t hammult_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec,
-                                int64_t vstride, int pass, cudaStream_t st);
+                                int64_t vstride, int pass, cudaStream_t st, double2 shift = double2{0.0, 0.0});
 
 // One-electron H (NELEC=1): KEMULT1 + V (hammod.F90:71-134).
 cudaError_t hammult1_launch(const HamDev &h, const double *vfull, const double2 *x, double2 *y,
@@ -86,6 +87,26 @@ cudaError_t dotdiag_launch(const double2 *const *a, const double2 *const *b, int
 // factor is also left in cout[0].  work as for gram (ticket at work[0]).
 cudaError_t gs_update_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
                              const double2 *d, int64_t len, double2 *work, double2 *cout, cudaStream_t st);
+
+// First pass of the fused two-pass Gram-Schmidt (m <= 16): q -= qp d,
+// v -= vp d with pass-1 coefficients d, and the pass-2 coefficients
+// <qp_i, q> reduced into dout[0..m) and |q|^2 into dout[64].  The second pass
+// is gs_pass2_launch with d2 = dout.
+cudaError_t gs_pass1_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
+                            const double2 *d, int64_t len, double2 *work, double2 *dout, cudaStream_t st);
+
+// Second pass: q <- (q - qp d2)/|w|, v <- (v - vp d2)/|w| with
+// |w|^2 = d2[64] - |d2[0..m)|^2; the factor also goes to cout[0].
+cudaError_t gs_pass2_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
+                            const double2 *d2, int64_t len, double2 *cout, cudaStream_t st);
+
+// k x k (k <= 16) dense helpers that keep the solver on the device.
+// flag bits: 1 Cholesky breakdown, 2 all-zero block, 4 orthonormality
+// self-check failed, 8 singular 1 x 1 Gram.
+cudaError_t small_cholinv_launch(const double2 *g, int k, double2 *rinv, int *flag, cudaStream_t st);
+cudaError_t small_hsqrt1_launch(const double2 *g, double2 *ginvh, double2 *gsq, int *flag, cudaStream_t st);
+cudaError_t small_ortho_check_launch(const double2 *t, int k, int *flag, cudaStream_t st);
+cudaError_t small_gemm_launch(const double2 *a, const double2 *b, double2 *c, int m, int k, int n, cudaStream_t st);
 
 // x_j *= c_j (c from DEVICE, complex), in place.
 cudaError_t scale_cols_launch(double2 *const *x, int n, const double2 *c_dev, int64_t len,

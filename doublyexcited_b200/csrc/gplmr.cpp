@@ -52,7 +52,9 @@ struct Solver {
     double2 *X = nullptr, *AX = nullptr, *W = nullptr, *AW = nullptr;
     double2 *S = nullptr, *AS = nullptr, *P = nullptr, *AP = nullptr;
     double2 *LV = nullptr, *LQ = nullptr;  // inner solve: order*nev each
-    double2 *dG = nullptr, *dC = nullptr, *dE = nullptr, *dR = nullptr, *dT = nullptr;
+    double2 *dG = nullptr, *dC = nullptr, *dE = nullptr, *dR = nullptr, *dT = nullptr, *dT2 = nullptr;
+    double2 *dRinv = nullptr, *dGinvh = nullptr, *dGsq = nullptr, *dG1 = nullptr, *dSV = nullptr;
+    int *dFlags = nullptr;
     double2 *hbuf = nullptr;  // pinned 64 x 128
     std::vector<double2 *> allocs;
 
@@ -95,7 +97,19 @@ struct Solver {
         DE_TRY(alloc(&dE, 64));
         DE_TRY(alloc(&dR, 64));
         DE_TRY(alloc(&dT, 64));
-        DE_CUDA(cudaMallocHost(&hbuf, 64 * 128 * sizeof(double2)));
+        DE_TRY(alloc(&dT2, 65));
+        DE_TRY(alloc(&dRinv, 16 * 16));
+        DE_TRY(alloc(&dGinvh, 16 * 16));
+        DE_TRY(alloc(&dGsq, 16 * 16));
+        DE_TRY(alloc(&dG1, 64 * 16));
+        DE_TRY(alloc(&dSV, 64 * 16));
+        {
+            double2 *f = nullptr;
+            DE_TRY(alloc(&f, 4));
+            dFlags = reinterpret_cast<int *>(f);
+            DE_CUDA(cudaMemsetAsync(dFlags, 0, 4 * sizeof(double2), st));
+        }
+        DE_CUDA(cudaMallocHost(&hbuf, (64 * 128 + 64) * sizeof(double2)));
         const int64_t wk = std::max<int64_t>(gram_work_elems(64, 128, D), dotdiag_work_elems(64, D));
         DE_TRY(h->ensure_work(wk));
         return DE_OK;
@@ -127,6 +141,20 @@ struct Solver {
         return DE_OK;
     }
 
+    // (H - sigma) x in one matvec (fused shift); compat mode keeps the
+    // reference's first-column-only product followed by the subtraction.
+    int inner_mult_shifted(const double2 *x, double2 *y, int k)
+    {
+        if (compat) {
+            DE_TRY(inner_mult(x, y, k));
+            return shift_sub(y, x, k);
+        }
+        mv_exec += k;
+        mv_ref += k;
+        const cplx ms = -sigma;
+        return h->matblock(x, y, k, make_double2(ms.real(), ms.imag()));
+    }
+
     static ColList cols(double2 *base, int k, int64_t D, double2 *sub = nullptr, cplx sg = 0.0)
     {
         ColList L{};
@@ -150,7 +178,10 @@ struct Solver {
     {
         DE_TRY(gram_dev(L, R, dG, L.n));
         DE_CUDA(cudaMemcpyAsync(hbuf, dG, (size_t)L.n * R.n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        int *hf = reinterpret_cast<int *>(hbuf + (size_t)L.n * R.n);
+        DE_CUDA(cudaMemcpyAsync(hf, dFlags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
         DE_CUDA(cudaStreamSynchronize(st));
+        DE_TRY(check_flags(hf[1]));  // an earlier device-side failure wins
         g.resize((size_t)L.n * R.n);
         for (size_t i = 0; i < g.size(); ++i) g[i] = cplx(hbuf[i].x, hbuf[i].y);
         return DE_OK;
@@ -205,26 +236,28 @@ struct Solver {
         return DE_OK;
     }
 
-    // cholQR lamod.f90:128-180; returns R (k x k upper) and applies X <- X R^{-1}.
-    int cholqr(double2 *x, int k, std::vector<cplx> &r)
+    // cholQR lamod.f90:128-180 on the device: R = chol(X^H X) (upper), X <- X
+    // R^{-1}; R^{-1} stays in dRinv for the following trsm.  Breakdown sets
+    // a device flag that the next residual check reports.
+    int cholqr(double2 *x, int k)
     {
-        DE_TRY(gram_host(cols(x, k, D), cols(x, k, D), r));
-        auto t0 = clk::now();
-        double rsum = 0.0;
-        for (auto &v : r) rsum += std::abs(v);
-        if (rsum == 0.0) return set_error(DE_E_CHOLESKY, "cholQR of an all-zero block (rsum=0)");
-        const int info = zpotrf_upper(k, r);
-        if (info == -1000) return set_error(DE_E_LAPACK, "host LAPACK not found (set DE_LAPACK_LIB)");
-        if (info != 0) return set_error(DE_E_CHOLESKY, "Cholesky failed!!! info=%d", info);
-        t_dense += secs(t0, clk::now());
-        return trsm(x, k, r);
+        DE_TRY(gram_dev(cols(x, k, D), cols(x, k, D), dG, k));
+        cudaError_t e = small_cholinv_launch(dG, k, dRinv, dFlags, st);
+        if (e != cudaSuccess) return cuda_error(e, "small_cholinv");
+        return trsm(x, k);
     }
 
-    // X <- X R^{-1} (ZTRSM 'R','U','N','N')
-    int trsm(double2 *x, int k, const std::vector<cplx> &r)
+    // X <- X R^{-1} (ZTRSM 'R','U','N','N') with the last cholqr's factor
+    int trsm(double2 *x, int k) { return update(cl(x, k), clw(x, k), dRinv, k, 1.0, 0.0); }
+
+    // report the first device flag raised by the k x k kernels
+    int check_flags(int flags)
     {
-        DE_TRY(upload(upper_inverse(k, r), dC));
-        return update(cl(x, k), clw(x, k), dC, k, 1.0, 0.0);
+        if (flags & 2) return set_error(DE_E_CHOLESKY, "cholQR of an all-zero block (rsum=0)");
+        if (flags & 1) return set_error(DE_E_CHOLESKY, "Cholesky failed!!! (cholQR breakdown)");
+        if (flags & 4) return set_error(DE_E_ORTHO, "AACK DOTS: inner-solve orthonormality self-check above 1e-10");
+        if (flags & 8) return set_error(DE_E_SVD, "inner-solve Gram matrix is singular");
+        return DE_OK;
     }
 
     // x_j <- x_j / ||x_j|| for two blocks sharing the factor (lamod normalize)
@@ -264,7 +297,9 @@ struct Solver {
             return cuda_error(e, "dotdiag");
         DE_CUDA(cudaMemcpyAsync(hbuf, dE, nev * sizeof(double2), cudaMemcpyDeviceToHost, st));
         DE_CUDA(cudaMemcpyAsync(hbuf + 64, dR, nev * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        DE_CUDA(cudaMemcpyAsync(hbuf + 128, dFlags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
         DE_CUDA(cudaStreamSynchronize(st));
+        DE_TRY(check_flags(reinterpret_cast<int *>(hbuf + 128)[1]));
         e_host.resize(nev);
         res.resize(nev);
         for (int j = 0; j < nev; ++j) {
@@ -283,9 +318,25 @@ struct Solver {
     int hgram(int m, double2 *q, double2 *v)
     {
         std::vector<const double2 *> qp = cl(LQ, m), vp = cl(LV, m);
+        cudaError_t e;
+        if (m == 0) {  // nothing to project: the two passes only normalise
+            e = gs_update_launch(qp.data(), vp.data(), 0, q, v, dT, D, h->d_work, dR, st);
+            if (e != cudaSuccess) return cuda_error(e, "gs_update");
+            return DE_OK;
+        }
+        if (m <= 16) {
+            // pass 1 with the pass-2 coefficients fused into its update; the
+            // intermediate normalisation of the reference cancels exactly.
+            DE_TRY(gram_dev(cols(LQ, m, D), cols(q, 1, D), dT, m));
+            e = gs_pass1_launch(qp.data(), vp.data(), m, q, v, dT, D, h->d_work, dT2, st);
+            if (e != cudaSuccess) return cuda_error(e, "gs_pass1");
+            e = gs_pass2_launch(qp.data(), vp.data(), m, q, v, dT2, D, dR, st);
+            if (e != cudaSuccess) return cuda_error(e, "gs_pass2");
+            return DE_OK;
+        }
         for (int pass = 0; pass < 2; ++pass) {
-            if (m > 0) DE_TRY(gram_dev(cols(LQ, m, D), cols(q, 1, D), dT, m));
-            cudaError_t e = gs_update_launch(qp.data(), vp.data(), m, q, v, dT, D, h->d_work, dR, st);
+            DE_TRY(gram_dev(cols(LQ, m, D), cols(q, 1, D), dT, m));
+            e = gs_update_launch(qp.data(), vp.data(), m, q, v, dT, D, h->d_work, dR, st);
             if (e != cudaSuccess) return cuda_error(e, "gs_update");
         }
         return DE_OK;
@@ -293,63 +344,65 @@ struct Solver {
 
     // basicblocklansolve harmonic_ritz_small.F90:258-324 on block b (k
     // columns), in place: b <- V (Q^H V_1) G^{1/2}.
-    int basic(double2 *b, int k)
+    int shift_sub(double2 *q, const double2 *v, int k)  // q <- q - sigma v
     {
         const cplx ms = -sigma;
-        const double2 msg = make_double2(ms.real(), ms.imag());
+        std::vector<double2 *> o = clw(q, k);
+        std::vector<const double2 *> a = cl(q, k), vv = cl(v, k);
+        cudaError_t e = axpc_launch(o.data(), a.data(), vv.data(), k, make_double2(ms.real(), ms.imag()), nullptr, D, st);
+        if (e != cudaSuccess) return cuda_error(e, "axpc");
+        return DE_OK;
+    }
+
+    int basic(double2 *b, int k)
+    {
         // harm_orthog_oneblock :161-244
         DE_CUDA(cudaMemcpyAsync(LV, b, (size_t)k * D * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-        DE_TRY(inner_mult(LV, LQ, k));
-        {
-            std::vector<double2 *> o = clw(LQ, k);
-            std::vector<const double2 *> a = cl(LQ, k), v = cl(LV, k);
-            cudaError_t e = axpc_launch(o.data(), a.data(), v.data(), k, msg, nullptr, D, st);
-            if (e != cudaSuccess) return cuda_error(e, "axpc");
+        DE_TRY(inner_mult_shifted(LV, LQ, k));
+        std::vector<cplx> gsq;
+        if (k == 1) {  // 1 x 1 Gram: its square roots on the device
+            DE_TRY(gram_dev(cols(LQ, 1, D), cols(LQ, 1, D), dG, 1));
+            cudaError_t e = small_hsqrt1_launch(dG, dGinvh, dGsq, dFlags, st);
+            if (e != cudaSuccess) return cuda_error(e, "small_hsqrt1");
+            DE_TRY(update(cl(LV, 1), clw(LV, 1), dGinvh, 1, 1.0, 0.0));
+        } else {
+            std::vector<cplx> g, ginv;
+            DE_TRY(gram_host(cols(LQ, k, D), cols(LQ, k, D), g));
+            auto t0 = clk::now();
+            DE_TRY(herm_sqrt_pair(k, g, ginv, gsq));
+            t_dense += secs(t0, clk::now());
+            std::vector<cplx> ginvh((size_t)k * k);
+            for (int j = 0; j < k; ++j)
+                for (int i = 0; i < k; ++i) ginvh[i + (size_t)k * j] = std::conj(ginv[j + (size_t)k * i]);
+            DE_TRY(upload(ginvh, dC));
+            DE_TRY(update(cl(LV, k), clw(LV, k), dC, k, 1.0, 0.0));
         }
-        std::vector<cplx> g, ginv, gsq;
-        DE_TRY(gram_host(cols(LQ, k, D), cols(LQ, k, D), g));
-        auto t0 = clk::now();
-        DE_TRY(herm_sqrt_pair(k, g, ginv, gsq));
-        t_dense += secs(t0, clk::now());
-        std::vector<cplx> ginvh((size_t)k * k);
-        for (int j = 0; j < k; ++j)
-            for (int i = 0; i < k; ++i) ginvh[i + (size_t)k * j] = std::conj(ginv[j + (size_t)k * i]);
-        DE_TRY(upload(ginvh, dC));
-        DE_TRY(update(cl(LV, k), clw(LV, k), dC, k, 1.0, 0.0));
         // self-check: (H - sigma) V_1 orthonormal to 1e-10
-        DE_TRY(inner_mult(LV, LQ, k));
+        DE_TRY(inner_mult_shifted(LV, LQ, k));
+        DE_TRY(gram_dev(cols(LQ, k, D), cols(LQ, k, D), dT, k));
         {
-            std::vector<double2 *> o = clw(LQ, k);
-            std::vector<const double2 *> a = cl(LQ, k), v = cl(LV, k);
-            cudaError_t e = axpc_launch(o.data(), a.data(), v.data(), k, msg, nullptr, D, st);
-            if (e != cudaSuccess) return cuda_error(e, "axpc");
+            cudaError_t e = small_ortho_check_launch(dT, k, dFlags, st);
+            if (e != cudaSuccess) return cuda_error(e, "small_ortho_check");
         }
-        std::vector<cplx> chk;
-        DE_TRY(gram_host(cols(LQ, k, D), cols(LQ, k, D), chk));
-        for (int j = 0; j < k; ++j)
-            for (int i = 0; i < k; ++i) {
-                const cplx v = chk[i + (size_t)k * j] - (i == j ? 1.0 : 0.0);
-                if (std::abs(v) > 1e-10) return set_error(DE_E_ORTHO, "AACK DOTS: |T(%d,%d)-I| = %.3e", i, j, std::abs(v));
-            }
         // fast_harmritz_setup :86-158 (maxiter = M^2 never truncates a block)
         for (int io = 0; io < order; ++io) {
             double2 *vb = col(LV, io * k), *qb = col(LQ, io * k);
-            if (io > 0) DE_TRY(inner_mult(col(LV, (io - 1) * k), vb, k));
             if (io > 0) {
-                DE_TRY(inner_mult(vb, qb, k));
+                DE_TRY(inner_mult(col(LV, (io - 1) * k), vb, k));
+                DE_TRY(inner_mult_shifted(vb, qb, k));
             } else {
                 mv_ref += compat ? 1 : k;  // the reference recomputes the product checked above
-            }
-            if (io > 0) {
-                std::vector<double2 *> o = clw(qb, k);
-                std::vector<const double2 *> a = cl(qb, k), v = cl(vb, k);
-                cudaError_t e = axpc_launch(o.data(), a.data(), v.data(), k, msg, nullptr, D, st);
-                if (e != cudaSuccess) return cuda_error(e, "axpc");
             }
             for (int i = 0; i < k; ++i) DE_TRY(hgram(io * k + i, col(qb, i), col(vb, i)));
         }
         // solution: V (lanham rhs), rhs(:,1,:) = G^{1/2} (:309-316)
         const int thisdim = order * k;
+        if (k == 1) {
+            DE_TRY(gram_dev(cols(LQ, thisdim, D), cols(LV, 1, D), dG1, thisdim));
+            cudaError_t e = small_gemm_launch(dG1, dGsq, dSV, thisdim, 1, 1, st);
+            if (e != cudaSuccess) return cuda_error(e, "small_gemm");
+            return update(cl(LV, thisdim), clw(b, 1), dSV, thisdim, 1.0, 0.0);
+        }
         std::vector<cplx> g1;  // Q^H V_1, thisdim x k (first block column of lanham)
         DE_TRY(gram_host(cols(LQ, thisdim, D), cols(LV, k, D), g1));
         std::vector<cplx> sv((size_t)thisdim * k, 0.0);
@@ -400,20 +453,19 @@ struct Solver {
             fflush(stdout);
         }
         int it = 1;
-        std::vector<cplx> R;
         while (it <= maxit && maxres > tol) {
-            DE_TRY(cholqr(X, nev, R));
-            DE_TRY(trsm(AX, nev, R));
+            DE_TRY(cholqr(X, nev));
+            DE_TRY(trsm(AX, nev));
             if (gm.max_inner_iter > 0) DE_TRY(precblock(W, nev));
             DE_TRY(orth_against(X, nev, W, nev));
-            DE_TRY(cholqr(W, nev, R));
+            DE_TRY(cholqr(W, nev));
             DE_TRY(matblock(W, AW, nev));
             if (ns > 0) {
                 DE_TRY(minus_e(S, AW, W, nev));
                 if (gm.max_inner_iter > 0) DE_TRY(precblock(S, nev));
                 DE_TRY(orth_against(X, nev, S, nev));
                 DE_TRY(orth_against(W, nev, S, nev));
-                DE_TRY(cholqr(S, nev, R));
+                DE_TRY(cholqr(S, nev));
                 DE_TRY(matblock(S, AS, nev));
                 for (int l = 2; l <= ns; ++l) {
                     const int j1 = (l - 1) * nev;
@@ -423,7 +475,7 @@ struct Solver {
                     DE_TRY(orth_against(X, nev, sl, nev));
                     DE_TRY(orth_against(W, nev, sl, nev));
                     DE_TRY(orth_against(S, j1, sl, nev));
-                    DE_TRY(cholqr(sl, nev, R));
+                    DE_TRY(cholqr(sl, nev));
                     DE_TRY(matblock(sl, asl, nev));
                 }
             }
@@ -431,8 +483,8 @@ struct Solver {
                 DE_TRY(orth_against(X, nev, P, nev, AX, AP));
                 DE_TRY(orth_against(W, nev, P, nev, AW, AP));
                 if (ldr > 0) DE_TRY(orth_against(S, ldr, P, nev, AS, AP));
-                DE_TRY(cholqr(P, nev, R));
-                DE_TRY(trsm(AP, nev, R));
+                DE_TRY(cholqr(P, nev));
+                DE_TRY(trsm(AP, nev));
             }
             // harmonic projection: K = B^H B, M = B^H V, B = A V - sigma V
             const int kdim = (it > 1) ? nproj : nproj - nev;

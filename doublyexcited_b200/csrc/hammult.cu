@@ -129,6 +129,8 @@ struct CubeArgs {
     double2 *y;
     int64_t vstride;
     const double *vfull;  // kOneElec: real V (length M)
+    double2 shd;          // diagonal shift added to V (cube kernel)
+    double2 shs;          // the same shift times SCALE^2 (streaming kernel)
 };
 
 // Owner phase of the group starting at slab K0: k-axis contraction for the
@@ -173,7 +175,7 @@ __device__ __forceinline__ void owner_group(const HamDev &h, const CubeArgs &a, 
                 constexpr int W = 2 * NN - 1;
                 const double vr = (h.t1a[e] + h.t1a[c]) +
                                   h.v12[(i - ip + NN - 1) + W * ((j - jp + NN - 1) + W * (k - kp + NN - 1))];
-                const double pr = vr * h.vsre, pi = vr * h.vsim;
+                const double pr = vr * h.vsre + a.shd.x, pi = vr * h.vsim + a.shd.y;
                 const double2 xe = xs[e];
                 yr += pr * xe.x - pi * xe.y;
                 yi += pr * xe.y + pi * xe.x;
@@ -185,7 +187,7 @@ __device__ __forceinline__ void owner_group(const HamDev &h, const CubeArgs &a, 
                 dst = make_double2(old.x + yr, old.y + yi);
             } else {
                 const double vr = a.vfull[e];
-                const double pr = vr * h.vsre, pi = vr * h.vsim;
+                const double pr = vr * h.vsre + a.shd.x, pi = vr * h.vsim + a.shd.y;
                 const double2 xe = xs[e];
                 yr += pr * xe.x - pi * xe.y;
                 yi += pr * xe.y + pi * xe.x;
@@ -411,7 +413,7 @@ __device__ __forceinline__ void stream_groups(const HamDev &h, const CubeArgs &a
                     const int e = t + P2 * l;
                     const double vr = (h.t1a[e] + t1p) +
                                       h.v12[(oi - ip + NN - 1) + W * ((oj - jp + NN - 1) + W * (l - kp + NN - 1))];
-                    const double pr = vr * h.sre, pi = vr * h.sim;
+                    const double pr = vr * h.sre + a.shs.x, pi = vr * h.sim + a.shs.y;
                     ar[l] += pr * v.x - pi * v.y;
                     ai[l] += pr * v.y + pi * v.x;
                 }
@@ -544,11 +546,20 @@ cudaError_t dispatch(const HamDev &h, const CubeArgs &a, int64_t ncubes, cudaStr
 
 }  // namespace
 
+static CubeArgs make_args(const HamDev &h, const double2 *x, double2 *y, int64_t vstride, double2 shift)
+{
+    CubeArgs a{x, y, vstride, nullptr, shift, make_double2(0.0, 0.0)};
+    // shift * SCALE^2 = shift / (1/SCALE^2)
+    const double s2r = h.sre * h.sre - h.sim * h.sim, s2i = 2.0 * h.sre * h.sim;
+    a.shs = make_double2(shift.x * s2r - shift.y * s2i, shift.x * s2i + shift.y * s2r);
+    return a;
+}
+
 cudaError_t hammult_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,
-                           cudaStream_t st)
+                           cudaStream_t st, double2 shift)
 {
     if (h.nelec != 2 || nvec <= 0) return cudaErrorInvalidValue;
-    CubeArgs a{x, y, vstride, nullptr};
+    const CubeArgs a = make_args(h, x, y, vstride, shift);
     const int64_t ncubes = h.m * (int64_t)nvec;
     if (ncubes > 0x7fffffffLL) return cudaErrorInvalidValue;
     cudaError_t e = dispatch<kRowsPot>(h, a, ncubes, st);
@@ -557,10 +568,10 @@ cudaError_t hammult_launch(const HamDev &h, const double2 *x, double2 *y, int nv
 }
 
 cudaError_t hammult_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,
-                                int pass, cudaStream_t st)
+                                int pass, cudaStream_t st, double2 shift)
 {
     if (h.nelec != 2 || nvec <= 0) return cudaErrorInvalidValue;
-    CubeArgs a{x, y, vstride, nullptr};
+    const CubeArgs a = make_args(h, x, y, vstride, shift);
     const int64_t ncubes = h.m * (int64_t)nvec;
     if (ncubes > 0x7fffffffLL) return cudaErrorInvalidValue;
     return pass == 0 ? dispatch<kRowsPot>(h, a, ncubes, st) : dispatch<kColsAcc>(h, a, ncubes, st);
@@ -570,7 +581,7 @@ cudaError_t hammult1_launch(const HamDev &h, const double *vfull, const double2 
                             int nvec, int64_t vstride, cudaStream_t st)
 {
     if (h.nelec != 1 || nvec <= 0) return cudaErrorInvalidValue;
-    CubeArgs a{x, y, vstride, vfull};
+    CubeArgs a{x, y, vstride, vfull, make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
     return dispatch<kOneElec>(h, a, nvec, st);
 }
 

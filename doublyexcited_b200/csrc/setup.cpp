@@ -238,30 +238,6 @@ std::vector<double> getinverse(int nout, int nbig, int nsmall, double delta)
 
 // ---------------------------------------------------------------- dense
 
-int zpotrf_upper(int k, std::vector<cplx> &a)
-{
-    const Lapack &L = lapack();
-    if (!L.ok) return -1000;
-    int info = 0;
-    L.zpotrf("U", &k, a.data(), &k, &info, 1);
-    for (int j = 0; j < k; ++j)
-        for (int i = j + 1; i < k; ++i) a[i + (size_t)k * j] = 0.0;
-    return info;
-}
-
-std::vector<cplx> upper_inverse(int k, const std::vector<cplx> &r)
-{
-    std::vector<cplx> inv((size_t)k * k, 0.0);
-    for (int j = 0; j < k; ++j) {  // solve R x = e_j by back substitution
-        for (int i = j; i >= 0; --i) {
-            cplx s = (i == j) ? 1.0 : 0.0;
-            for (int l = i + 1; l <= j; ++l) s -= r[i + (size_t)k * l] * inv[l + (size_t)k * j];
-            inv[i + (size_t)k * j] = s / r[i + (size_t)k * i];
-        }
-    }
-    return inv;
-}
-
 int herm_sqrt_pair(int k, const std::vector<cplx> &g, std::vector<cplx> &ginv,
                    std::vector<cplx> &gsq)
 {
