@@ -68,8 +68,8 @@ def alg_bytes(nn):
     return 32 * nn ** 6
 
 
-# dram bytes (read + write) per vector-matvec (pass A + pass B) from the ncu
-# capture summarised in profiles/stream_kernel_n6.md; None until captured.
+# dram bytes (read + write) per vector-matvec (pass A + pass B), keyed by
+# (NN, storage), from the ncu captures summarised under profiles/.
 NCU_TRAFFIC_PER_VECTOR = {}
 
 
@@ -140,6 +140,31 @@ def fp64_peak_tflops(torch):
     return 2 * n ** 3 / best / 1e12
 
 
+def fp32_peak_tflops(torch):
+    """Measured FP32 CUDA-core peak: cuBLAS SGEMM 8192^3 with TF32 off, best
+    of 5 -- the compute denominator of the FP32 matvec roofline."""
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
+    return 2 * n ** 3 / best / 1e12
+
+
 def cpu_matvec_seconds(w, reps):
     """Seconds per oracle HAMMULT (C, OpenMP over columns, all host cores)."""
     from oracle import oracle as O  # CPU baseline only
@@ -204,6 +229,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="solve-n6", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="mixed: FP32 inner solve, FP64 outer iteration (the product form); fp64: plain")
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="skip the plain-FP64 solves timed beside the mixed ones")
     a = ap.parse_args()
     w = WORKLOADS[a.workload]
     if a.impl == "reference":
@@ -231,15 +260,6 @@ def main():
             pg.barrier()
 
     nn = 2 * w["n"] + 1
-    prob = de.Problem(n=w["n"], delta=w["delta"], theta=w["theta"], device=local)
-    stream = torch.cuda.current_stream()
-    prob.set_stream(stream.cuda_stream)
-    x0 = seeded_start(prob.m, w["nev"], w["seed"], w["spin"])
-    dim = prob.dim
-    x0_dev = torch.from_numpy(np.ascontiguousarray(x0.T)).to("cuda")  # (nev, dim): columns contiguous
-    x_dev = torch.empty_like(x0_dev)
-    e_host = np.empty(w["nev"], np.complex128)
-
     import ctypes
 
     from doublyexcited_b200._lib import check, de_complex, de_gmres, de_stats, lib
@@ -247,46 +267,72 @@ def main():
     L = lib()
     gm = de_gmres(w["order"], 1, 1e-3, 0)
     sig = de_complex(w["sigma"], 0.0)
+    stream = torch.cuda.current_stream()
 
-    def solve_dev():
-        x_dev.copy_(x0_dev)
-        st = de_stats()
-        check(L.de_gplmr_eig_d(prob.handle, ctypes.c_void_p(x_dev.data_ptr()), ctypes.c_void_p(e_host.ctypes.data),
-                               prob.m, dim // prob.m, sig, w["nev"], w["ns"], w["maxit"], w["tol"], ctypes.byref(gm), 0,
-                               ctypes.byref(st)), "de_gplmr_eig_d")
-        return st
+    def measure(precision, sample_clocks):
+        """W untimed + K timed solves at one precision, device-timed."""
+        prob = de.Problem(n=w["n"], delta=w["delta"], theta=w["theta"], device=local, precision=precision)
+        prob.set_stream(stream.cuda_stream)
+        x0 = seeded_start(prob.m, w["nev"], w["seed"], w["spin"])
+        dim = prob.dim
+        x0_dev = torch.from_numpy(np.ascontiguousarray(x0.T)).to("cuda")  # (nev, dim): columns contiguous
+        x_dev = torch.empty_like(x0_dev)
+        e_host = np.empty(w["nev"], np.complex128)
 
-    for _ in range(a.warmup):
-        st = solve_dev()
-    torch.cuda.synchronize()
-    barrier()
-    sampler = ClockSampler(local)
-    sampler.start()
-    prob.set_profiling(True)
-    prob.profile_read()
-    torch.cuda.synchronize()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = L.de_kernel_launches()
-    e0.record(stream)
-    stats = []
-    for _ in range(a.steps):
-        stats.append(solve_dev())
-    e1.record(stream)
-    launches = L.de_kernel_launches() - launches0
-    torch.cuda.synchronize()
-    elapsed = e0.elapsed_time(e1) / 1e3
-    barrier()
-    clocks = sampler.stop()
-    prof = prob.profile_read()
-    prob.set_profiling(False)
-    if pg:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        elapsed = float(t.item())
-    value = a.steps * world / elapsed
-    st = stats[-1]
-    e_final = complex(e_host[0])
+        def solve_dev():
+            x_dev.copy_(x0_dev)
+            st = de_stats()
+            check(L.de_gplmr_eig_d(prob.handle, ctypes.c_void_p(x_dev.data_ptr()),
+                                   ctypes.c_void_p(e_host.ctypes.data), prob.m, dim // prob.m, sig, w["nev"],
+                                   w["ns"], w["maxit"], w["tol"], ctypes.byref(gm), 0, ctypes.byref(st)),
+                  "de_gplmr_eig_d")
+            return st
+
+        for _ in range(a.warmup):
+            solve_dev()
+        torch.cuda.synchronize()
+        barrier()
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+        prob.set_profiling(True)
+        prob.profile_read()
+        prob.profile_read32()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = L.de_kernel_launches()
+        e0.record(stream)
+        stats = []
+        for _ in range(a.steps):
+            stats.append(solve_dev())
+        e1.record(stream)
+        launches = L.de_kernel_launches() - launches0
+        torch.cuda.synchronize()
+        elapsed = e0.elapsed_time(e1) / 1e3
+        barrier()
+        clocks = sampler.stop() if sampler else None
+        prof = prob.profile_read()
+        prof32 = prob.profile_read32()
+        prob.set_profiling(False)
+        if pg:
+            t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            elapsed = float(t.item())
+        out = {"prob": prob, "x0": x0, "dim": dim, "elapsed": elapsed, "stats": stats, "st": stats[-1],
+               "e": complex(e_host[0]), "e_all": e_host.copy(), "prof": prof, "prof32": prof32,
+               "launches": launches,
+               "clocks": clocks, "value": a.steps * world / elapsed}
+        del x_dev, x0_dev
+        return out
+
+    head = measure(a.precision, True)
+    other = measure("fp64", False) if a.precision != "fp64" and not a.no_fp64_compare else None
+    prob, x0, dim = head["prob"], head["x0"], head["dim"]
+    elapsed, st, e_final, prof, launches, clocks = (head["elapsed"], head["st"], head["e"], head["prof"],
+                                                     head["launches"], head["clocks"])
+    value = head["value"]
+    e_host = np.empty(w["nev"], np.complex128)
 
     # end to end through the host-pointer C ABI (pinned host buffers)
     x_pin = torch.from_numpy(np.asfortranarray(x0).reshape(-1, order="F").view(np.float64)).pin_memory()
@@ -313,10 +359,32 @@ def main():
     e2e = e2e_steps * world / t_e2e
 
     peak = fp64_peak_tflops(torch)
-    mv_ms = prof["pass_a_ms"] + prof["pass_b_ms"]
-    vecs = max(1, prof["vectors"])
-    achieved = alg_flops(nn) * vecs / (mv_ms / 1e3) / 1e12 if mv_ms > 0 else 0.0
-    traffic = NCU_TRAFFIC_PER_VECTOR.get(nn)
+    peak32 = fp32_peak_tflops(torch)
+
+    def roof(pr, fp32, pk, src):
+        ms = pr["pass_a_ms"] + pr["pass_b_ms"]
+        vecs = max(1, pr["vectors"])
+        ach = alg_flops(nn) * vecs / (ms / 1e3) / 1e12 if ms > 0 else 0.0
+        ebytes = 16 if fp32 else 32
+        return {"bound": "tensor" if not fp32 else "fp32-fma", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                "frac": ach / pk if pk else None,
+                "traffic": NCU_TRAFFIC_PER_VECTOR.get((nn, "f32" if fp32 else "f64")),
+                "kernel": f"hammult stream_kernel<{'float' if fp32 else 'double'}> pass A + pass B, per vector-matvec",
+                "alg_flops_per_vector": alg_flops(nn), "alg_bytes_per_vector": ebytes * nn ** 6,
+                "achieved_gbs_alg": ebytes * nn ** 6 * vecs / (ms / 1e3) / 1e9 if ms > 0 else None,
+                "matvec_ms_per_vector": ms / vecs, "pass_a_ms": pr["pass_a_ms"] / vecs,
+                "pass_b_ms": pr["pass_b_ms"] / vecs, "vectors": pr["vectors"], "device_ms_total": ms,
+                "peak_source": src}
+
+    src64 = "FP64 dense peak measured in this run: cuBLAS DGEMM 8192^3 (no FP64 entry in MEASURED_PEAKS.json)"
+    src32 = "FP32 CUDA-core peak measured in this run: cuBLAS SGEMM 8192^3 with TF32 off"
+    roof64 = roof(prof, False, peak, src64)
+    roof32 = roof(head["prof32"], True, peak32, src32) if head["prof32"]["vectors"] else None
+    # the dominant kernel of the run heads the line
+    if roof32 and roof32["device_ms_total"] > roof64["device_ms_total"]:
+        roofline, roofline_other = roof32, roof64
+    else:
+        roofline, roofline_other = roof64, roof32
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -326,31 +394,33 @@ def main():
                "sample": f"3 oracle HAMMULTs at N={w['n']} (C, OpenMP over columns, {cores} threads) "
                          f"= {t_mv:.3f} s each, x {nmv} HAMMULTs per solve; block ops not charged"}
 
+    compare = None
+    if other is not None:
+        de_max = float(np.max(np.abs(np.sort_complex(head["e_all"]) - np.sort_complex(other["e_all"]))))
+        compare = {"fp64_value": other["value"], "fp64_ms_per_step": other["elapsed"] / a.steps * 1e3,
+                   "fp64_iterations": other["st"].iterations, "fp64_E": [other["e"].real, other["e"].imag],
+                   "speedup_vs_fp64": value / other["value"], "dE_vs_fp64": de_max}
+        other["prob"].close()
+
     if rank == 0:
         line = {
             "metric": "resonance solves/s", "value": value, "unit": "solves/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": elapsed / a.steps * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if a.precision == "fp64" else "f32 inner solve / f64 outer iteration",
             "data": "synthetic (seeded complex-Gaussian singlet start vector; operator from the reference's physics)",
             "config": {"workload": a.workload, "N": w["n"], "NN": nn, "dim": dim, "nev": w["nev"], "ns": w["ns"],
                        "order": w["order"], "theta": w["theta"], "delta": w["delta"], "sigma": w["sigma"],
-                       "tol": w["tol"], "precision": "fp64",
+                       "tol": w["tol"], "precision": a.precision,
                        "l2": "inputs larger than L2 (GPLMR workspace "
                              f"{(17 + 2 * w['order']) * w['nev'] * dim * 16 / 1e9:.1f} GB per solve)",
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": int(x0.nbytes),
                     "d2h_bytes_per_step": int(x0.nbytes + e_host.nbytes)},
-            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak if peak else None,
-                         "traffic": traffic,
-                         "kernel": "hammult stream_kernel pass A + pass B (FP64), per vector-matvec",
-                         "alg_flops_per_vector": alg_flops(nn), "alg_bytes_per_vector": alg_bytes(nn),
-                         "achieved_gbs_alg": alg_bytes(nn) * vecs / (mv_ms / 1e3) / 1e9 if mv_ms > 0 else None,
-                         "matvec_ms_per_vector": mv_ms / vecs, "pass_a_ms": prof["pass_a_ms"] / vecs,
-                         "pass_b_ms": prof["pass_b_ms"] / vecs,
-                         "peak_source": "FP64 dense peak measured in this run: cuBLAS DGEMM 8192^3 (no FP64 "
-                                        "entry in MEASURED_PEAKS.json)"},
+            "roofline": roofline,
+            "roofline_other_matvec": roofline_other,
             "cpu_baseline": cpu,
+            "mixed_vs_fp64": compare,
             "gpu_launches": int(launches),
             "clocks": clocks,
             "solve": {"iterations": st.iterations, "converged": bool(st.converged), "E": [e_final.real, e_final.imag],

@@ -14,6 +14,8 @@ mirroring the reference's entry points (paths relative to
 * :meth:`Problem.gplmr_eig` -- ``GPLMR_EIG`` gplmr.F90:9-374
 * :func:`read_input`        -- ``get_input``/``get_args`` input.F90:143-362
 * :func:`write_vectors` / :func:`read_vectors` -- utils.F90:82-198
+* :class:`Server` -- many independent solves on one GPU (no reference
+  counterpart): admission by device footprint, concurrent streams
 
 There is no CPU fallback: if the library is missing or no GPU is present the
 calls raise.
@@ -22,11 +24,14 @@ from __future__ import annotations
 
 from ._lib import (  # noqa: F401
     DE_E_CHOLESKY,
+    DE_E_CUDA,
+    DE_E_NOMEM,
     DE_E_GEVP,
     DE_E_INVALID,
     DE_E_IO,
     DE_E_LAPACK,
     DE_E_NAN,
+    DE_E_BUSY,
     DE_E_ORTHO,
     DE_E_PARSE,
     DE_E_SIZE,
@@ -36,11 +41,13 @@ from ._lib import (  # noqa: F401
     lib,
     lib_path,
 )
-from .api import Problem, GplmrResult, read_input, read_vectors, vectors_header, write_vectors  # noqa: F401
+from .api import Problem, GplmrResult, Server, ServedResult, read_input, read_vectors, vectors_header, write_vectors  # noqa: F401,E501
 
 __all__ = [
     "Problem",
     "GplmrResult",
+    "Server",
+    "ServedResult",
     "read_input",
     "read_vectors",
     "vectors_header",

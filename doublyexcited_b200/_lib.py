@@ -95,6 +95,37 @@ class de_input(ctypes.Structure):
     ]
 
 
+class de_server_opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_int), ("max_bytes", ctypes.c_int64)]
+
+
+class de_request(ctypes.Structure):
+    _fields_ = [
+        ("params", de_params),
+        ("sigma", de_complex),
+        ("nev", ctypes.c_int),
+        ("ns", ctypes.c_int),
+        ("maxit", ctypes.c_int),
+        ("tol", ctypes.c_double),
+        ("gm", de_gmres),
+        ("x", ctypes.c_void_p),
+        ("e", ctypes.c_void_p),
+    ]
+
+
+class de_result(ctypes.Structure):
+    _fields_ = [
+        ("id", ctypes.c_uint64),
+        ("status", ctypes.c_int),
+        ("stats", de_stats),
+        ("t_submit_s", ctypes.c_double),
+        ("t_start_s", ctypes.c_double),
+        ("t_end_s", ctypes.c_double),
+        ("footprint_bytes", ctypes.c_int64),
+        ("worker", ctypes.c_int),
+    ]
+
+
 class DeError(RuntimeError):
     """A non-zero status from the C ABI."""
 
@@ -121,10 +152,13 @@ SIGNATURES = {
     "de_set_profiling": (INT, [P, INT]),
     "de_profile_read": (INT, [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                               ctypes.POINTER(I64), ctypes.POINTER(I64)]),
+    "de_profile_read32": (INT, [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                ctypes.POINTER(I64), ctypes.POINTER(I64)]),
     "de_hammult": (INT, [P, P, P, I64]),
     "de_hammult_d": (INT, [P, P, P, I64]),
     "de_matblock": (INT, [P, P, P, I64, I64, INT]),
     "de_matblock_d": (INT, [P, P, P, I64, I64, INT]),
+    "de_matblock32_d": (INT, [P, P, P, I64, I64, INT]),
     "de_dots": (INT, [P, P, P, I64, INT, INT, P, INT]),
     "de_dots_d": (INT, [P, P, P, I64, INT, INT, P, INT]),
     "de_dots_noalloc_d": (INT, [P, P, I64, INT, INT, P, INT, P]),
@@ -139,6 +173,15 @@ SIGNATURES = {
     "de_write_vectors": (INT, [ctypes.c_char_p, I64, INT, P]),
     "de_read_vectors": (INT, [ctypes.c_char_p, I64, INT, P]),
     "de_vectors_header": (INT, [ctypes.c_char_p, ctypes.POINTER(I64), ctypes.POINTER(INT)]),
+    "de_request_footprint": (INT, [ctypes.POINTER(de_request), ctypes.POINTER(I64)]),
+    "de_server_create": (INT, [ctypes.POINTER(de_server_opts), ctypes.POINTER(P)]),
+    "de_server_submit": (INT, [P, ctypes.POINTER(de_request), ctypes.POINTER(ctypes.c_uint64)]),
+    "de_server_wait": (INT, [P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(de_result)]),
+    "de_server_wait_any": (INT, [P, ctypes.c_double, ctypes.POINTER(de_result)]),
+    "de_server_now": (ctypes.c_double, [P]),
+    "de_server_load": (INT, [P, ctypes.POINTER(INT), ctypes.POINTER(INT), ctypes.POINTER(I64)]),
+    "de_server_destroy": (INT, [P]),
+    "de_problem_trim": (INT, [P]),
 }
 
 _LIB = None

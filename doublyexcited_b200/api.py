@@ -9,6 +9,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
+from . import _lib as _l
 from ._lib import check, de_complex, de_gmres, de_input, de_params, de_stats, lib
 
 
@@ -43,14 +44,21 @@ class GplmrResult:
 
 class Problem:
     """One operator instance (HAMILTONIAN + PARAMETERS of the reference) on
-    one GPU.  Mirrors ``INIT_STRUCTS``/``INIT_HAMILTONIAN``."""
+    one GPU.  Mirrors ``INIT_STRUCTS``/``INIT_HAMILTONIAN``.  precision
+    "fp64" is the plain form; "mixed" runs the eigensolver's inner solve
+    (PRECBLOCK_BASIC) in complex64 with FP32 matvecs while the outer
+    iteration, its residuals and every MATBLOCK stay FP64."""
 
     def __init__(self, n: int, delta: float = 2.0, theta: float = 0.2, charge: float = 2.0,
                  nelec: int = 2, nsmall: int = 22, tfactor: int = 4, device: int = 0,
-                 autodelta: bool = False, radius: float = 7.0):
+                 autodelta: bool = False, radius: float = 7.0, precision: str = "fp64"):
         L = lib()
         p = de_params()
         L.de_params_default(ctypes.byref(p))
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        p.precision = 1 if precision == "mixed" else 0
+        self.precision = precision
         p.n, p.delta, p.theta, p.charge = n, delta, theta, charge
         p.nelec, p.nsmall, p.tfactor, p.device = nelec, nsmall, tfactor, device
         p.autodelta, p.radius = int(bool(autodelta)), radius
@@ -103,6 +111,14 @@ class Problem:
               "de_profile_read")
         return {"pass_a_ms": a.value, "pass_b_ms": b.value, "calls": c.value, "vectors": v.value}
 
+    def profile_read32(self) -> dict:
+        """The same for the FP32 matvecs of the mixed form's inner solve."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        c, v = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().de_profile_read32(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(v)),
+              "de_profile_read32")
+        return {"pass_a_ms": a.value, "pass_b_ms": b.value, "calls": c.value, "vectors": v.value}
+
     # -- operator ---------------------------------------------------------
     def hammult(self, x: np.ndarray) -> np.ndarray:
         x = _block(x, self.dim)[:, 0].copy()
@@ -121,6 +137,12 @@ class Problem:
         """Device-pointer MATBLOCK (e.g. torch tensors' data_ptr())."""
         check(lib().de_matblock_d(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), self.m,
                                   self.dim // self.m, nev), "de_matblock_d")
+
+    def matblock32_d(self, x_ptr: int, y_ptr: int, nev: int) -> None:
+        """Device-pointer MATBLOCK on complex64 vectors in FP32 arithmetic (the
+        mixed form's inner-solve matvec)."""
+        check(lib().de_matblock32_d(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), self.m,
+                                    self.dim // self.m, nev), "de_matblock32_d")
 
     def dots(self, bras: np.ndarray, kets: np.ndarray, hermitian: bool = True) -> np.ndarray:
         b = _block(bras, bras.shape[0])
@@ -207,3 +229,113 @@ def vectors_header(path: str) -> tuple[int, int]:
     n = ctypes.c_int()
     check(lib().de_vectors_header(path.encode(), ctypes.byref(m), ctypes.byref(n)), "de_vectors_header")
     return m.value, n.value
+
+
+# -- batched and served solves ---------------------------------------------------
+
+@dataclass
+class ServedResult:
+    id: int
+    status: int
+    e: np.ndarray
+    x: np.ndarray
+    iterations: int
+    converged: bool
+    max_residual: float
+    t_submit_s: float
+    t_start_s: float
+    t_end_s: float
+    footprint_bytes: int
+    worker: int
+    tag: object = None
+
+    @property
+    def latency_s(self) -> float:
+        return self.t_end_s - self.t_submit_s
+
+
+class Server:
+    """Many independent GPLMR solves on one GPU (``de_server_*``): requests
+    are admitted first come, first served when a worker is free and their
+    device footprint fits in ``max_bytes``; each worker runs its solves on
+    its own CUDA stream, so different solves overlap on the device."""
+
+    def __init__(self, workers: int = 4, max_bytes: int = 0, device: int = 0):
+        o = _l.de_server_opts(device, workers, max_bytes)
+        h = ctypes.c_void_p()
+        check(lib().de_server_create(ctypes.byref(o), ctypes.byref(h)), "de_server_create")
+        self._h = h
+        self._live = {}  # id -> (request, x, e, tag): buffers stay alive until collected
+
+    @staticmethod
+    def request(n: int, x0: np.ndarray, sigma: complex, *, theta: float = 0.2, delta: float = 2.0,
+                charge: float = 2.0, precision: str = "fp64", ns: int = 5, maxit: int = 100, tol: float = 1e-7,
+                max_inner_iter: int = 5):
+        p = de_params()
+        lib().de_params_default(ctypes.byref(p))
+        p.n, p.delta, p.theta, p.charge = n, delta, theta, charge
+        p.precision = 1 if precision == "mixed" else 0
+        x = np.array(x0, dtype=np.complex128, order="F", copy=True)
+        if x.ndim == 1:
+            x = x[:, None]
+        e = np.empty(x.shape[1], np.complex128)
+        r = _l.de_request(p, de_complex(complex(sigma).real, complex(sigma).imag), x.shape[1], ns, maxit, tol,
+                          de_gmres(max_inner_iter, 1, 1e-3, 0), x.ctypes.data, e.ctypes.data)
+        return r, x, e
+
+    @staticmethod
+    def footprint(req) -> int:
+        b = ctypes.c_int64()
+        check(lib().de_request_footprint(ctypes.byref(req[0]), ctypes.byref(b)), "de_request_footprint")
+        return b.value
+
+    def submit(self, req, tag=None) -> int:
+        r, x, e = req
+        i = ctypes.c_uint64()
+        check(lib().de_server_submit(self._h, ctypes.byref(r), ctypes.byref(i)), "de_server_submit")
+        self._live[i.value] = (r, x, e, tag)
+        return i.value
+
+    def _result(self, res) -> ServedResult:
+        r, x, e, tag = self._live.pop(res.id)
+        st = res.stats
+        return ServedResult(res.id, res.status, e, x, st.iterations, bool(st.converged), st.max_residual,
+                            res.t_submit_s, res.t_start_s, res.t_end_s, res.footprint_bytes, res.worker, tag)
+
+    def wait(self, rid: int, timeout_s: float = -1.0) -> ServedResult:
+        res = _l.de_result()
+        check(lib().de_server_wait(self._h, rid, timeout_s, ctypes.byref(res)), "de_server_wait")
+        return self._result(res)
+
+    def wait_any(self, timeout_s: float = -1.0) -> ServedResult | None:
+        res = _l.de_result()
+        s = lib().de_server_wait_any(self._h, timeout_s, ctypes.byref(res))
+        if s == _l.DE_E_BUSY:
+            return None
+        check(s, "de_server_wait_any")
+        return self._result(res)
+
+    def now(self) -> float:
+        return lib().de_server_now(self._h)
+
+    def load(self) -> tuple[int, int, int]:
+        q, r, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64()
+        check(lib().de_server_load(self._h, ctypes.byref(q), ctypes.byref(r), ctypes.byref(b)), "de_server_load")
+        return q.value, r.value, b.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().de_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -11,6 +11,8 @@
 //
 // Every kernel here streams its vectors once; they are HBM-bound except the
 // 64 x 64 projection Gram, which is FP64-FMA bound (8 flops per complex MAC).
+// The vector kernels are templated on the storage type S (double2, or
+// float2 for the mixed form's inner solve); sums always accumulate in FP64.
 #include "de_internal.h"
 #include "de_kernels.h"
 
@@ -37,20 +39,48 @@ constexpr int kGramRT = 32;  // rows per smem tile
 constexpr int kSmallBlocks = 296;  // grid of the fused small reductions
 constexpr int kGramTX = 16;  // thread grid 16 x 16
 
-__device__ __forceinline__ double2 col_elem(const ColList &L, int c, int64_t r)
+// element load widened to FP64
+__device__ __forceinline__ double2 ld2(const double2 *p) { return __ldg(p); }
+__device__ __forceinline__ double2 ld2(const float2 *p)
 {
-    double2 v = __ldg(L.a[c] + r);
+    const float2 v = __ldg(p);
+    return make_double2(v.x, v.y);
+}
+// plain (coherent) loads, for data the same kernel may have written
+__device__ __forceinline__ double2 ldp(const double2 *p) { return *p; }
+__device__ __forceinline__ double2 ldp(const float2 *p)
+{
+    const float2 v = *p;
+    return make_double2(v.x, v.y);
+}
+template <class S>
+__device__ __forceinline__ S st2(double x, double y);
+template <>
+__device__ __forceinline__ double2 st2<double2>(double x, double y)
+{
+    return make_double2(x, y);
+}
+template <>
+__device__ __forceinline__ float2 st2<float2>(double x, double y)
+{
+    return make_float2((float)x, (float)y);
+}
+
+template <class S>
+__device__ __forceinline__ double2 col_elem(const ColListT<S> &L, int c, int64_t r)
+{
+    double2 v = ld2(L.a[c] + r);
     if (L.b[c] != nullptr) {
-        const double2 w = __ldg(L.b[c] + r);
+        const double2 w = ld2(L.b[c] + r);
         v.x -= L.sigma.x * w.x - L.sigma.y * w.y;
         v.y -= L.sigma.x * w.y + L.sigma.y * w.x;
     }
     return v;
 }
 
-template <int TA, int TB>
+template <class S, int TA, int TB>
 __global__ void __launch_bounds__(256)
-    gram_partial(const __grid_constant__ ColList L, const __grid_constant__ ColList R, int64_t len,
+    gram_partial(const __grid_constant__ ColListT<S> L, const __grid_constant__ ColListT<S> R, int64_t len,
                  int64_t chunk, int herm, double2 *__restrict__ work)
 {
     extern __shared__ double2 gsm[];
@@ -117,20 +147,32 @@ __global__ void __launch_bounds__(256)
         }
 }
 
-__global__ void gram_reduce(const double2 *__restrict__ work, int nblk, int nl, int nr,
-                            double2 *__restrict__ out, int ldo)
+// One 256-thread block per 32 outputs; warp g sums blocks b = g (mod 8).
+__global__ void __launch_bounds__(256)
+    gram_reduce(const double2 *__restrict__ work, int nblk, int nl, int nr, double2 *__restrict__ out, int ldo)
 {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= nl * nr) return;
-    double sr = 0.0, si = 0.0;
-    const int64_t stride = (int64_t)nl * nr;
-    for (int b = 0; b < nblk; ++b) {
-        const double2 v = work[b * stride + o];
-        sr += v.x;
-        si += v.y;
+    __shared__ double2 acc[8][32];
+    const int g = threadIdx.x >> 5, lane = threadIdx.x & 31, o = blockIdx.x * 32 + lane;
+    const int nout = nl * nr;
+    double sx = 0.0, sy = 0.0;
+    if (o < nout) {
+#pragma unroll 8
+        for (int b = g; b < nblk; b += 8) {
+            const double2 v = work[(int64_t)b * nout + o];
+            sx += v.x;
+            sy += v.y;
+        }
     }
-    const int i = o % nl, j = o / nl;
-    out[i + (int64_t)ldo * j] = make_double2(sr, si);
+    acc[g][lane] = make_double2(sx, sy);
+    __syncthreads();
+    if (threadIdx.x < 32 && o < nout) {
+        double x = 0.0, y = 0.0;
+        for (int k = 0; k < 8; ++k) {
+            x += acc[k][threadIdx.x].x;
+            y += acc[k][threadIdx.x].y;
+        }
+        out[o % nl + (int64_t)ldo * (o / nl)] = make_double2(x, y);
+    }
 }
 
 int gram_blocks(int nl, int nr, int64_t len)
@@ -140,8 +182,8 @@ int gram_blocks(int nl, int nr, int64_t len)
     return (int)std::max<int64_t>(1, std::min(tiles, cap));
 }
 
-template <int TA, int TB>
-cudaError_t gram_go(const ColList &L, const ColList &R, int64_t len, int herm, double2 *work,
+template <int TA, int TB, class S>
+cudaError_t gram_go(const ColListT<S> &L, const ColListT<S> &R, int64_t len, int herm, double2 *work,
                     int nblk, int64_t chunk, cudaStream_t st)
 {
     const size_t smem = (size_t)kGramRT * (L.n + R.n) * sizeof(double2);
@@ -150,13 +192,13 @@ cudaError_t gram_go(const ColList &L, const ColList &R, int64_t len, int herm, d
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!attr[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(gram_partial<TA, TB>,
+        cudaError_t e = cudaFuncSetAttribute(gram_partial<S, TA, TB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)(kGramRT * (64 + 128) * sizeof(double2)));
         if (e != cudaSuccess) return e;
         attr[dev] = true;
     }
-    gram_partial<TA, TB><<<nblk, 256, smem, st>>>(L, R, len, chunk, herm, work);
+    gram_partial<S, TA, TB><<<nblk, 256, smem, st>>>(L, R, len, chunk, herm, work);
     count_launch();
     return cudaGetLastError();
 }
@@ -169,9 +211,9 @@ int round_t(int n)
 
 // ---------------------------------------------------------------- update
 
-template <int NOUT>
+template <class SI, class SO, int NOUT>
 __global__ void __launch_bounds__(256)
-    update_kernel(const __grid_constant__ UpdList U, const double2 *__restrict__ C, int ldc,
+    update_kernel(const __grid_constant__ UpdListT<SI, SO> U, const double2 *__restrict__ C, int ldc,
                   int64_t len)
 {
     extern __shared__ double2 cs[];  // [nin][NOUT]
@@ -188,10 +230,10 @@ __global__ void __launch_bounds__(256)
         for (int j = 0; j < NOUT; ++j) {
             acc[j] = make_double2(0.0, 0.0);
             yb[j] = make_double2(0.0, 0.0);
-            if (j < nout && (U.beta[j].x != 0.0 || U.beta[j].y != 0.0)) yb[j] = cmul(U.beta[j], U.y[j][r]);
+            if (j < nout && (U.beta[j].x != 0.0 || U.beta[j].y != 0.0)) yb[j] = cmul(U.beta[j], ldp(U.y[j] + r));
         }
         for (int i = 0; i < nin; ++i) {
-            const double2 xv = U.x[i][r];
+            const double2 xv = ldp(U.x[i] + r);
 #pragma unroll
             for (int j = 0; j < NOUT; ++j) {
                 const double2 c = cs[i * NOUT + j];
@@ -204,18 +246,18 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int j = 0; j < NOUT; ++j) {
             const double2 s = cmul(U.alpha, acc[j]);
-            if (j < nout) U.y[j][r] = make_double2(yb[j].x + s.x, yb[j].y + s.y);
+            if (j < nout) U.y[j][r] = st2<SO>(yb[j].x + s.x, yb[j].y + s.y);
         }
     }
 }
 
-template <int NOUT>
-cudaError_t update_go(const UpdList &U, const double2 *c, int ldc, int64_t len, cudaStream_t st)
+template <int NOUT, class SI, class SO>
+cudaError_t update_go(const UpdListT<SI, SO> &U, const double2 *c, int ldc, int64_t len, cudaStream_t st)
 {
     const size_t smem = (size_t)U.nin * NOUT * sizeof(double2);
     const int64_t want = (len + 255) / 256;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, 148 * 8));
-    update_kernel<NOUT><<<blocks, 256, smem, st>>>(U, c, ldc, len);
+    update_kernel<SI, SO, NOUT><<<blocks, 256, smem, st>>>(U, c, ldc, len);
     count_launch();
     return cudaGetLastError();
 }
@@ -287,18 +329,34 @@ __global__ void dotdiag_partial(const __grid_constant__ PtrPack P, int64_t len, 
     }
 }
 
-__global__ void dotdiag_reduce(const double2 *__restrict__ work, int nblk, int n,
-                               double2 *__restrict__ out)
+// One 256-thread block per output j: strided partial sums, then a fixed
+// shuffle/shared-memory tree (deterministic).
+__global__ void __launch_bounds__(256)
+    dotdiag_reduce(const double2 *__restrict__ work, int nblk, int n, double2 *__restrict__ out)
 {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
+    __shared__ double2 acc[8];
+    const int j = blockIdx.x;
     double sr = 0.0, si = 0.0;
-    for (int b = 0; b < nblk; ++b) {
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
         const double2 v = work[(int64_t)j * nblk + b];
         sr += v.x;
         si += v.y;
     }
-    out[j] = make_double2(sr, si);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        sr += __shfl_down_sync(0xffffffffu, sr, off);
+        si += __shfl_down_sync(0xffffffffu, si, off);
+    }
+    if ((threadIdx.x & 31) == 0) acc[threadIdx.x >> 5] = make_double2(sr, si);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0.0, y = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            x += acc[k].x;
+            y += acc[k].y;
+        }
+        out[j] = make_double2(x, y);
+    }
 }
 
 __global__ void inv_sqrt_abs_kernel(const double2 *d, double2 *c, int n)
@@ -381,11 +439,43 @@ __device__ __forceinline__ void block_sum(double (&re)[N], double (&im)[N], doub
     }
 }
 
+// Final sum of nblk per-block partials part[b*stride + o], o < nout <= 32,
+// by the whole 256-thread block in a fixed order: warp g sums the blocks
+// b = g (mod 8) for every output, then one thread per output adds the 8
+// warp sums.  Eight independent load chains instead of one thread's serial
+// chain over all partials; the result does not depend on block timing.
+__device__ __forceinline__ void reduce_partials(const double2 *__restrict__ part, unsigned nblk, int stride,
+                                                int nout, double2 *res)
+{
+    __shared__ double2 acc[8][32];
+    const int g = threadIdx.x >> 5, o = threadIdx.x & 31;
+    double sx = 0.0, sy = 0.0;
+    if (o < nout) {
+#pragma unroll 8
+        for (unsigned b = g; b < nblk; b += 8) {
+            const double2 v = __ldcg(part + (int64_t)b * stride + o);
+            sx += v.x;
+            sy += v.y;
+        }
+    }
+    acc[g][o] = make_double2(sx, sy);
+    __syncthreads();
+    if ((int)threadIdx.x < nout) {
+        double x = 0.0, y = 0.0;
+        for (int k = 0; k < 8; ++k) {
+            x += acc[k][threadIdx.x].x;
+            y += acc[k][threadIdx.x].y;
+        }
+        res[threadIdx.x] = make_double2(x, y);
+    }
+    __syncthreads();
+}
+
 // G = op(L)^T R for nl*nr <= NLM*NRM <= 32, register accumulation over a
 // grid-stride loop of rows, fused reduction.
-template <int NLM, int NRM>
+template <class S, int NLM, int NRM>
 __global__ void __launch_bounds__(256)
-    gram_small(const __grid_constant__ ColList L, const __grid_constant__ ColList R, int64_t len, int herm,
+    gram_small(const __grid_constant__ ColListT<S> L, const __grid_constant__ ColListT<S> R, int64_t len, int herm,
                double2 *__restrict__ work, double2 *__restrict__ out, int ldo)
 {
     const int nl = L.n, nr = R.n;
@@ -419,16 +509,11 @@ __global__ void __launch_bounds__(256)
     const int nout = NLM * NRM;
     block_sum<NLM * NRM>(ar, ai, part + (int64_t)blockIdx.x * nout, nout);
     if (last_block(ticket, gridDim.x)) {
+        __shared__ double2 res[32];
+        reduce_partials(part, gridDim.x, nout, nout, res);
         for (int o = threadIdx.x; o < nl * nr; o += blockDim.x) {
             const int i = o / nr, j = o % nr;
-            const int k = i * NRM + j;
-            double a = 0.0, b = 0.0;
-            for (unsigned bb = 0; bb < gridDim.x; ++bb) {
-                const double2 v = __ldcg(part + (int64_t)bb * nout + k);
-                a += v.x;
-                b += v.y;
-            }
-            out[i + (int64_t)ldo * j] = make_double2(a, b);
+            out[i + (int64_t)ldo * j] = res[i * NRM + j];
         }
         if (threadIdx.x == 0) *ticket = 0u;
     }
@@ -437,15 +522,17 @@ __global__ void __launch_bounds__(256)
 // Gram-Schmidt step of myhgramschmidt_many (harmonic_ritz_small.F90:52-59):
 //   q -= sum_i Qp_i d_i ; v -= sum_i Vp_i d_i ; c = 1/sqrt(|<q,q>|)
 // with d (m values) and the output c in device memory.
+template <class S>
 struct GsArgs {
-    const double2 *qp[64];
-    const double2 *vp[64];
-    double2 *q, *v;
+    const S *qp[64];
+    const S *vp[64];
+    S *q, *v;
     int m;
 };
 
+template <class S>
 __global__ void __launch_bounds__(256)
-    gs_update(const __grid_constant__ GsArgs A, const double2 *__restrict__ d, int64_t len,
+    gs_update(const __grid_constant__ GsArgs<S> A, const double2 *__restrict__ d, int64_t len,
               double2 *__restrict__ work, double2 *__restrict__ cout)
 {
     __shared__ double2 ds[64];
@@ -454,50 +541,53 @@ __global__ void __launch_bounds__(256)
     double nr[1] = {0.0}, ni[1] = {0.0};
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
-        double2 q = A.q[r], v = A.v[r];
+        double2 q = ldp(A.q + r), v = ldp(A.v + r);
         for (int i = 0; i < A.m; ++i) {
             const double2 c = ds[i];
-            const double2 a = A.qp[i][r], b = A.vp[i][r];
+            const double2 a = ldp(A.qp[i] + r), b = ldp(A.vp[i] + r);
             q.x -= a.x * c.x - a.y * c.y;
             q.y -= a.x * c.y + a.y * c.x;
             v.x -= b.x * c.x - b.y * c.y;
             v.y -= b.x * c.y + b.y * c.x;
         }
-        A.q[r] = q;
-        A.v[r] = v;
-        nr[0] = fma(q.x, q.x, nr[0]);
-        nr[0] = fma(q.y, q.y, nr[0]);
+        const S qs = st2<S>(q.x, q.y);
+        A.q[r] = qs;
+        A.v[r] = st2<S>(v.x, v.y);
+        const double2 qr = ldp(&qs);  // the norm of the stored vector
+        nr[0] = fma(qr.x, qr.x, nr[0]);
+        nr[0] = fma(qr.y, qr.y, nr[0]);
     }
     unsigned *ticket = reinterpret_cast<unsigned *>(work);
     double2 *part = work + 1;
     block_sum<1>(nr, ni, part + blockIdx.x, 1);
     if (last_block(ticket, gridDim.x)) {
+        __shared__ double2 res[32];
+        reduce_partials(part, gridDim.x, 1, 1, res);
         if (threadIdx.x == 0) {
-            double a = 0.0;
-            for (unsigned bb = 0; bb < gridDim.x; ++bb) a += __ldcg(part + bb).x;
-            cout[0] = make_double2(1.0 / sqrt(fabs(a)), 0.0);
+            cout[0] = make_double2(1.0 / sqrt(fabs(res[0].x)), 0.0);
             *ticket = 0u;
         }
     }
 }
 
-__global__ void gs_scale(double2 *__restrict__ q, double2 *__restrict__ v, const double2 *__restrict__ c, int64_t len)
+template <class S>
+__global__ void gs_scale(S *__restrict__ q, S *__restrict__ v, const double2 *__restrict__ c, int64_t len)
 {
     const double s = c[0].x;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
-        const double2 a = q[r], b = v[r];
-        q[r] = make_double2(a.x * s, a.y * s);
-        v[r] = make_double2(b.x * s, b.y * s);
+        const double2 a = ldp(q + r), b = ldp(v + r);
+        q[r] = st2<S>(a.x * s, a.y * s);
+        v[r] = st2<S>(b.x * s, b.y * s);
     }
 }
 
 // Second pass of the fused two-pass Gram-Schmidt: with the pass-1
 // coefficients d (device), q -= Qp d and v -= Vp d, then the pass-2
 // coefficients <Qp_i, q> (i < m) are reduced into dout (m values).
-template <int MM>
+template <class S, int MM>
 __global__ void __launch_bounds__(256)
-    gs_pass1(const __grid_constant__ GsArgs A, const double2 *__restrict__ d, int64_t len,
+    gs_pass1(const __grid_constant__ GsArgs<S> A, const double2 *__restrict__ d, int64_t len,
              double2 *__restrict__ work, double2 *__restrict__ dout)
 {
     __shared__ double2 ds[64];
@@ -508,22 +598,26 @@ __global__ void __launch_bounds__(256)
     for (int i = 0; i <= MM; ++i) ar[i] = ai[i] = 0.0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
-        double2 q = A.q[r], v = A.v[r];
+        double2 q = ldp(A.q + r), v = ldp(A.v + r);
         double2 a[MM];
 #pragma unroll
         for (int i = 0; i < MM; ++i) {
             if (i < A.m) {
                 const double2 c = ds[i];
-                a[i] = A.qp[i][r];
-                const double2 b = A.vp[i][r];
+                a[i] = ldp(A.qp[i] + r);
+                const double2 b = ldp(A.vp[i] + r);
                 q.x -= a[i].x * c.x - a[i].y * c.y;
                 q.y -= a[i].x * c.y + a[i].y * c.x;
                 v.x -= b.x * c.x - b.y * c.y;
                 v.y -= b.x * c.y + b.y * c.x;
             }
         }
-        A.q[r] = q;
-        A.v[r] = v;
+        {
+            const S qs = st2<S>(q.x, q.y);
+            A.q[r] = qs;
+            A.v[r] = st2<S>(v.x, v.y);
+            q = ldp(&qs);  // coefficients of the stored vector
+        }
 #pragma unroll
         for (int i = 0; i < MM; ++i) {
             if (i < A.m) {  // conj(a_i) q
@@ -540,17 +634,10 @@ __global__ void __launch_bounds__(256)
     double2 *part = work + 1;
     block_sum<MM + 1>(ar, ai, part + (int64_t)blockIdx.x * (MM + 1), MM + 1);
     if (last_block(ticket, gridDim.x)) {
-        for (int o = threadIdx.x; o <= MM; o += blockDim.x) {
-            if (o < A.m || o == MM) {
-                double x = 0.0, y = 0.0;
-                for (unsigned bb = 0; bb < gridDim.x; ++bb) {
-                    const double2 w = __ldcg(part + (int64_t)bb * (MM + 1) + o);
-                    x += w.x;
-                    y += w.y;
-                }
-                dout[o == MM ? 64 : o] = make_double2(x, y);  // |u|^2 goes to dout[64]
-            }
-        }
+        __shared__ double2 res[32];
+        reduce_partials(part, gridDim.x, MM + 1, MM + 1, res);
+        for (int o = threadIdx.x; o <= MM; o += blockDim.x)
+            if (o < A.m || o == MM) dout[o == MM ? 64 : o] = res[o];  // |u|^2 goes to dout[64]
         if (threadIdx.x == 0) *ticket = 0u;
     }
 }
@@ -559,8 +646,9 @@ __global__ void __launch_bounds__(256)
 // v <- (v - Vp d2)/|w| where |w|^2 = |u|^2 - |d2|^2 (Pythagoras; u is the
 // pass-1 vector, whose component in span(Qp) is already at rounding level,
 // so the subtraction loses nothing).
+template <class S>
 __global__ void __launch_bounds__(256)
-    gs_pass2(const __grid_constant__ GsArgs A, const double2 *__restrict__ d2, int64_t len, double2 *cout)
+    gs_pass2(const __grid_constant__ GsArgs<S> A, const double2 *__restrict__ d2, int64_t len, double2 *cout)
 {
     __shared__ double2 ds[64];
     __shared__ double scale;
@@ -575,17 +663,17 @@ __global__ void __launch_bounds__(256)
     const double sc = scale;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
-        double2 q = A.q[r], v = A.v[r];
+        double2 q = ldp(A.q + r), v = ldp(A.v + r);
         for (int i = 0; i < A.m; ++i) {
             const double2 c = ds[i];
-            const double2 a = A.qp[i][r], b = A.vp[i][r];
+            const double2 a = ldp(A.qp[i] + r), b = ldp(A.vp[i] + r);
             q.x -= a.x * c.x - a.y * c.y;
             q.y -= a.x * c.y + a.y * c.x;
             v.x -= b.x * c.x - b.y * c.y;
             v.y -= b.x * c.y + b.y * c.x;
         }
-        A.q[r] = make_double2(q.x * sc, q.y * sc);
-        A.v[r] = make_double2(v.x * sc, v.y * sc);
+        A.q[r] = st2<S>(q.x * sc, q.y * sc);
+        A.v[r] = st2<S>(v.x * sc, v.y * sc);
     }
 }
 
@@ -665,13 +753,13 @@ __global__ void small_hsqrt1(const double2 *__restrict__ g, double2 *__restrict_
 
 // harm_orthog_oneblock's self-check (harmonic_ritz_small.F90:221-242):
 // flag |= 4 when any |T - I| > 1e-10.
-__global__ void small_ortho_check(const double2 *__restrict__ t, int k, int *flag)
+__global__ void small_ortho_check(const double2 *__restrict__ t, int k, double tol, int *flag)
 {
     const int o = threadIdx.x;
     if (o < k * k) {
         const int i = o % k, j = o / k;
         const double re = t[o].x - (i == j ? 1.0 : 0.0);
-        if (!(hypot(re, t[o].y) <= 1e-10)) raise_flag(flag, 4);
+        if (!(hypot(re, t[o].y) <= tol)) raise_flag(flag, 4);
     }
 }
 
@@ -691,6 +779,21 @@ __global__ void small_gemm(const double2 *__restrict__ A, const double2 *__restr
     C[o] = s;
 }
 
+__global__ void cvt_c2f_kernel(const double2 *__restrict__ x, float2 *__restrict__ y, int64_t n)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double2 v = x[i];
+        y[i] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
+__global__ void cvt_r2f_kernel(const double *__restrict__ x, float *__restrict__ y, int64_t n)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) y[i] = (float)x[i];
+}
+
 int stream_blocks(int64_t len)
 {
     return (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, 148 * 4));
@@ -703,21 +806,22 @@ int64_t gram_work_elems(int nl, int nr, int64_t len)
     return 1 + std::max<int64_t>((int64_t)gram_blocks(nl, nr, len) * nl * nr, (int64_t)kSmallBlocks * 32);
 }
 
-template <int A, int B>
-static cudaError_t gram_small_go(const ColList &L, const ColList &R, int64_t len, int herm, double2 *out, int ldo,
-                                 double2 *work, cudaStream_t st)
+template <int A, int B, class S>
+static cudaError_t gram_small_go(const ColListT<S> &L, const ColListT<S> &R, int64_t len, int herm, double2 *out,
+                                 int ldo, double2 *work, cudaStream_t st)
 {
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, kSmallBlocks));
-    gram_small<A, B><<<blocks, 256, 0, st>>>(L, R, len, herm, work, out, ldo);
+    gram_small<S, A, B><<<blocks, 256, 0, st>>>(L, R, len, herm, work, out, ldo);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t gs_update_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
-                             const double2 *d, int64_t len, double2 *work, double2 *cout, cudaStream_t st)
+template <class S>
+static cudaError_t gs_update_go(const S *const *qp, const S *const *vp, int m, S *q, S *v, const double2 *d,
+                                int64_t len, double2 *work, double2 *cout, cudaStream_t st)
 {
     if (m < 0 || m > 64) return cudaErrorInvalidValue;
-    GsArgs A{};
+    GsArgs<S> A{};
     for (int i = 0; i < m; ++i) {
         A.qp[i] = qp[i];
         A.vp[i] = vp[i];
@@ -726,17 +830,30 @@ cudaError_t gs_update_launch(const double2 *const *qp, const double2 *const *vp,
     A.v = v;
     A.m = m;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, kSmallBlocks));
-    gs_update<<<blocks, 256, 0, st>>>(A, d, len, work, cout);
+    gs_update<S><<<blocks, 256, 0, st>>>(A, d, len, work, cout);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    gs_scale<<<blocks, 256, 0, st>>>(q, v, cout, len);
+    gs_scale<S><<<blocks, 256, 0, st>>>(q, v, cout, len);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t gram_launch(const ColList &L, const ColList &R, int64_t len, int herm, double2 *out,
-                        int ldo, double2 *work, cudaStream_t st)
+cudaError_t gs_update_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
+                             const double2 *d, int64_t len, double2 *work, double2 *cout, cudaStream_t st)
+{
+    return gs_update_go(qp, vp, m, q, v, d, len, work, cout, st);
+}
+
+cudaError_t gs_update_launch(const float2 *const *qp, const float2 *const *vp, int m, float2 *q, float2 *v,
+                             const double2 *d, int64_t len, double2 *work, double2 *cout, cudaStream_t st)
+{
+    return gs_update_go(qp, vp, m, q, v, d, len, work, cout, st);
+}
+
+template <class S>
+static cudaError_t gram_any(const ColListT<S> &L, const ColListT<S> &R, int64_t len, int herm, double2 *out, int ldo,
+                            double2 *work, cudaStream_t st)
 {
     if (L.n < 1 || L.n > 64 || R.n < 1 || R.n > 128 || len < 1) return cudaErrorInvalidValue;
     if (R.n == 1 && L.n <= 32) {
@@ -767,13 +884,25 @@ cudaError_t gram_launch(const ColList &L, const ColList &R, int64_t len, int her
 #undef GRAM_CASE
     if (e != cudaSuccess) return e;
     const int nout = L.n * R.n;
-    gram_reduce<<<(nout + 255) / 256, 256, 0, st>>>(work, nblk, L.n, R.n, out, ldo);
+    gram_reduce<<<(nout + 31) / 32, 256, 0, st>>>(work, nblk, L.n, R.n, out, ldo);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t update_launch(const UpdList &U, const double2 *c_dev, int ldc, int64_t len,
-                          cudaStream_t st)
+cudaError_t gram_launch(const ColList &L, const ColList &R, int64_t len, int herm, double2 *out, int ldo,
+                        double2 *work, cudaStream_t st)
+{
+    return gram_any(L, R, len, herm, out, ldo, work, st);
+}
+
+cudaError_t gram_launch(const ColListF &L, const ColListF &R, int64_t len, int herm, double2 *out, int ldo,
+                        double2 *work, cudaStream_t st)
+{
+    return gram_any(L, R, len, herm, out, ldo, work, st);
+}
+
+template <class SI, class SO>
+static cudaError_t update_any(const UpdListT<SI, SO> &U, const double2 *c_dev, int ldc, int64_t len, cudaStream_t st)
 {
     if (U.nin < 1 || U.nin > kMaxCols || U.nout < 1 || U.nout > 16 || len < 1)
         return cudaErrorInvalidValue;
@@ -782,6 +911,21 @@ cudaError_t update_launch(const UpdList &U, const double2 *c_dev, int ldc, int64
     if (U.nout <= 4) return update_go<4>(U, c_dev, ldc, len, st);
     if (U.nout <= 8) return update_go<8>(U, c_dev, ldc, len, st);
     return update_go<16>(U, c_dev, ldc, len, st);
+}
+
+cudaError_t update_launch(const UpdList &U, const double2 *c_dev, int ldc, int64_t len, cudaStream_t st)
+{
+    return update_any(U, c_dev, ldc, len, st);
+}
+cudaError_t update_launch(const UpdListT<float2, float2> &U, const double2 *c_dev, int ldc, int64_t len,
+                          cudaStream_t st)
+{
+    return update_any(U, c_dev, ldc, len, st);
+}
+cudaError_t update_launch(const UpdListT<float2, double2> &U, const double2 *c_dev, int ldc, int64_t len,
+                          cudaStream_t st)
+{
+    return update_any(U, c_dev, ldc, len, st);
 }
 
 cudaError_t axpc_launch(double2 *const *out, const double2 *const *a, const double2 *const *b,
@@ -831,16 +975,17 @@ cudaError_t dotdiag_launch(const double2 *const *a, const double2 *const *b, int
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    dotdiag_reduce<<<1, 64, 0, st>>>(work, nblk, n, out);
+    dotdiag_reduce<<<n, 256, 0, st>>>(work, nblk, n, out);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t gs_pass1_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
-                            const double2 *d, int64_t len, double2 *work, double2 *dout, cudaStream_t st)
+template <class S>
+static cudaError_t gs_pass1_go(const S *const *qp, const S *const *vp, int m, S *q, S *v, const double2 *d,
+                               int64_t len, double2 *work, double2 *dout, cudaStream_t st)
 {
     if (m < 1 || m > 16) return cudaErrorInvalidValue;
-    GsArgs A{};
+    GsArgs<S> A{};
     for (int i = 0; i < m; ++i) {
         A.qp[i] = qp[i];
         A.vp[i] = vp[i];
@@ -849,20 +994,32 @@ cudaError_t gs_pass1_launch(const double2 *const *qp, const double2 *const *vp, 
     A.v = v;
     A.m = m;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, kSmallBlocks));
-    if (m <= 1) gs_pass1<1><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
-    else if (m <= 2) gs_pass1<2><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
-    else if (m <= 4) gs_pass1<4><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
-    else if (m <= 8) gs_pass1<8><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
-    else gs_pass1<16><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+    if (m <= 1) gs_pass1<S, 1><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+    else if (m <= 2) gs_pass1<S, 2><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+    else if (m <= 4) gs_pass1<S, 4><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+    else if (m <= 8) gs_pass1<S, 8><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+    else gs_pass1<S, 16><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
     count_launch();
     return cudaGetLastError();
 }
 
-cudaError_t gs_pass2_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
-                            const double2 *d2, int64_t len, double2 *cout, cudaStream_t st)
+cudaError_t gs_pass1_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
+                            const double2 *d, int64_t len, double2 *work, double2 *dout, cudaStream_t st)
+{
+    return gs_pass1_go(qp, vp, m, q, v, d, len, work, dout, st);
+}
+cudaError_t gs_pass1_launch(const float2 *const *qp, const float2 *const *vp, int m, float2 *q, float2 *v,
+                            const double2 *d, int64_t len, double2 *work, double2 *dout, cudaStream_t st)
+{
+    return gs_pass1_go(qp, vp, m, q, v, d, len, work, dout, st);
+}
+
+template <class S>
+static cudaError_t gs_pass2_go(const S *const *qp, const S *const *vp, int m, S *q, S *v, const double2 *d2,
+                               int64_t len, double2 *cout, cudaStream_t st)
 {
     if (m < 1 || m > 64) return cudaErrorInvalidValue;
-    GsArgs A{};
+    GsArgs<S> A{};
     for (int i = 0; i < m; ++i) {
         A.qp[i] = qp[i];
         A.vp[i] = vp[i];
@@ -870,9 +1027,20 @@ cudaError_t gs_pass2_launch(const double2 *const *qp, const double2 *const *vp, 
     A.q = q;
     A.v = v;
     A.m = m;
-    gs_pass2<<<stream_blocks(len) * 2, 256, 0, st>>>(A, d2, len, cout);
+    gs_pass2<S><<<stream_blocks(len) * 2, 256, 0, st>>>(A, d2, len, cout);
     count_launch();
     return cudaGetLastError();
+}
+
+cudaError_t gs_pass2_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
+                            const double2 *d2, int64_t len, double2 *cout, cudaStream_t st)
+{
+    return gs_pass2_go(qp, vp, m, q, v, d2, len, cout, st);
+}
+cudaError_t gs_pass2_launch(const float2 *const *qp, const float2 *const *vp, int m, float2 *q, float2 *v,
+                            const double2 *d2, int64_t len, double2 *cout, cudaStream_t st)
+{
+    return gs_pass2_go(qp, vp, m, q, v, d2, len, cout, st);
 }
 
 cudaError_t small_cholinv_launch(const double2 *g, int k, double2 *rinv, int *flag, cudaStream_t st)
@@ -890,10 +1058,10 @@ cudaError_t small_hsqrt1_launch(const double2 *g, double2 *ginvh, double2 *gsq, 
     return cudaGetLastError();
 }
 
-cudaError_t small_ortho_check_launch(const double2 *t, int k, int *flag, cudaStream_t st)
+cudaError_t small_ortho_check_launch(const double2 *t, int k, int *flag, cudaStream_t st, double tol)
 {
     if (k < 1 || k > 16) return cudaErrorInvalidValue;
-    small_ortho_check<<<1, 256, 0, st>>>(t, k, flag);
+    small_ortho_check<<<1, 256, 0, st>>>(t, k, tol, flag);
     count_launch();
     return cudaGetLastError();
 }
@@ -910,6 +1078,22 @@ cudaError_t inv_sqrt_abs_launch(const double2 *d, double2 *c, int n, cudaStream_
 {
     if (n < 1 || n > 64) return cudaErrorInvalidValue;
     inv_sqrt_abs_kernel<<<1, 64, 0, st>>>(d, c, n);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t to_f32_launch(const double2 *x, float2 *y, int64_t n, cudaStream_t st)
+{
+    if (n < 1) return cudaErrorInvalidValue;
+    cvt_c2f_kernel<<<stream_blocks(n) * 2, 256, 0, st>>>(x, y, n);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t to_f32_launch(const double *x, float *y, int64_t n, cudaStream_t st)
+{
+    if (n < 1) return cudaErrorInvalidValue;
+    cvt_r2f_kernel<<<stream_blocks(n), 256, 0, st>>>(x, y, n);
     count_launch();
     return cudaGetLastError();
 }

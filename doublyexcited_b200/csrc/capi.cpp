@@ -95,15 +95,19 @@ std::shared_ptr<std::vector<double>> cached_tinv(int nout, int nbig, int nsmall,
 
 }  // namespace
 
+// Device buffers of a handle come from the stream-ordered allocator
+// (cudaMallocAsync / cudaFreeAsync on the handle's stream), so handles that
+// run side by side on one GPU never force a device-wide synchronisation
+// when they grow or release their workspace.
 int de_problem::ensure_stage(int64_t elems)
 {
     if (elems <= stage_elems) return DE_OK;
-    if (d_x) cudaFree(d_x);
-    if (d_y) cudaFree(d_y);
+    if (d_x) cudaFreeAsync(d_x, stream);
+    if (d_y) cudaFreeAsync(d_y, stream);
     d_x = d_y = nullptr;
     stage_elems = 0;
-    DE_CUDA(cudaMalloc(&d_x, elems * sizeof(double2)));
-    DE_CUDA(cudaMalloc(&d_y, elems * sizeof(double2)));
+    DE_CUDA(cudaMallocAsync(&d_x, elems * sizeof(double2), stream));
+    DE_CUDA(cudaMallocAsync(&d_y, elems * sizeof(double2), stream));
     stage_elems = elems;
     return DE_OK;
 }
@@ -111,13 +115,36 @@ int de_problem::ensure_stage(int64_t elems)
 int de_problem::ensure_work(int64_t elems)
 {
     if (elems <= work_elems) return DE_OK;
-    if (d_work) cudaFree(d_work);
+    if (d_work) cudaFreeAsync(d_work, stream);
     d_work = nullptr;
     work_elems = 0;
-    DE_CUDA(cudaMalloc(&d_work, elems * sizeof(double2)));
-    DE_CUDA(cudaMemset(d_work, 0, sizeof(double2)));  // reduction ticket
+    DE_CUDA(cudaMallocAsync(&d_work, elems * sizeof(double2), stream));
+    DE_CUDA(cudaMemsetAsync(d_work, 0, sizeof(double2), stream));  // reduction ticket
     work_elems = elems;
     return DE_OK;
+}
+
+void de_problem::trim()
+{
+    for (auto it = cache.begin(); it != cache.end();) {
+        if (!it->used) {
+            cudaFreeAsync(it->p, stream);
+            it = cache.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    if (d_x) cudaFreeAsync(d_x, stream);
+    if (d_y) cudaFreeAsync(d_y, stream);
+    d_x = d_y = nullptr;
+    stage_elems = 0;
+}
+
+int64_t de_problem::cached_bytes() const
+{
+    int64_t b = 0;
+    for (auto &c : cache) b += (int64_t)c.bytes;
+    return b + 2 * stage_elems * (int64_t)sizeof(double2) + work_elems * (int64_t)sizeof(double2);
 }
 
 void *de_problem::cache_get(size_t bytes)
@@ -130,18 +157,21 @@ void *de_problem::cache_get(size_t bytes)
         return best->p;
     }
     void *p = nullptr;
-    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    if (cudaMallocAsync(&p, bytes, stream) != cudaSuccess) {
         cudaGetLastError();
         // release idle blocks and retry once
         for (auto it = cache.begin(); it != cache.end();) {
             if (!it->used) {
-                cudaFree(it->p);
+                cudaFreeAsync(it->p, stream);
                 it = cache.erase(it);
             } else {
                 ++it;
             }
         }
-        if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+        if (cudaMallocAsync(&p, bytes, stream) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
     }
     cache.push_back(Blk{p, bytes, true});
     return p;
@@ -172,10 +202,10 @@ int de_problem::harvest()
         float a = 0.f, b = 0.f;
         DE_CUDA(cudaEventElapsedTime(&a, r.e[0], r.e[1]));
         DE_CUDA(cudaEventElapsedTime(&b, r.e[1], r.e[2]));
-        prof_ms[0] += a;
-        prof_ms[1] += b;
-        prof_calls += 1;
-        prof_vectors += r.nvec;
+        prof_ms[r.f32][0] += a;
+        prof_ms[r.f32][1] += b;
+        prof_calls[r.f32] += 1;
+        prof_vectors[r.f32] += r.nvec;
         for (auto ev : r.e) ev_free.push_back(ev);
     }
     ev_pending.clear();
@@ -189,23 +219,51 @@ int de_problem::matblock(const double2 *x, double2 *y, int nvec, double2 shift)
         if (e != cudaSuccess) return cuda_error(e, "hammult1");
         return DE_OK;
     }
-    Rec r{{nullptr, nullptr, nullptr}, nvec};
-    if (prof) {
-        for (auto &ev : r.e)
-            if (!(ev = take_event())) return set_error(DE_E_CUDA, "cudaEventCreate failed");
-        DE_CUDA(cudaEventRecord(r.e[0], stream));
-    }
+    Rec r{{nullptr, nullptr, nullptr}, nvec, 0};
+    DE_TRY(prof_begin(r));
     cudaError_t e = hammult_pass_launch(ham, x, y, nvec, dim, 0, stream, shift);
     if (e != cudaSuccess) return cuda_error(e, "hammult pass A");
-    if (prof) DE_CUDA(cudaEventRecord(r.e[1], stream));
+    DE_TRY(prof_mid(r));
     e = hammult_pass_launch(ham, x, y, nvec, dim, 1, stream);
     if (e != cudaSuccess) return cuda_error(e, "hammult pass B");
-    if (prof) {
-        DE_CUDA(cudaEventRecord(r.e[2], stream));
-        ev_pending.push_back(r);
-        if (ev_pending.size() > 4096) DE_TRY(harvest());
-    }
+    return prof_end(r);
+}
+
+int de_problem::prof_begin(Rec &r)
+{
+    if (!prof) return DE_OK;
+    for (auto &ev : r.e)
+        if (!(ev = take_event())) return set_error(DE_E_CUDA, "cudaEventCreate failed");
+    DE_CUDA(cudaEventRecord(r.e[0], stream));
     return DE_OK;
+}
+
+int de_problem::prof_mid(Rec &r)
+{
+    if (prof) DE_CUDA(cudaEventRecord(r.e[1], stream));
+    return DE_OK;
+}
+
+int de_problem::prof_end(Rec &r)
+{
+    if (!prof) return DE_OK;
+    DE_CUDA(cudaEventRecord(r.e[2], stream));
+    ev_pending.push_back(r);
+    if (ev_pending.size() > 4096) DE_TRY(harvest());
+    return DE_OK;
+}
+
+int de_problem::matblock32(const float2 *x, float2 *y, int nvec, double2 shift)
+{
+    if (p.nelec != 2) return set_error(DE_E_INVALID, "the FP32 matvec is built for the two-electron operator");
+    Rec r{{nullptr, nullptr, nullptr}, nvec, 1};
+    DE_TRY(prof_begin(r));
+    cudaError_t e = hammult_pass_launch(ham, x, y, nvec, dim, 0, stream, shift);
+    if (e != cudaSuccess) return cuda_error(e, "hammult FP32 pass A");
+    DE_TRY(prof_mid(r));
+    e = hammult_pass_launch(ham, x, y, nvec, dim, 1, stream);
+    if (e != cudaSuccess) return cuda_error(e, "hammult FP32 pass B");
+    return prof_end(r);
 }
 
 extern "C" {
@@ -221,6 +279,8 @@ DE_API int de_problem_create(const de_params *pin, de_problem **out)
     if (nn > 23)
         return set_error(DE_E_UNSUPPORTED, "N=%d: grids above NN=23 are not built in this version", p.n);
     if (p.nsmall < 1 || p.tfactor < 1) return set_error(DE_E_INVALID, "nsmall/tfactor must be positive");
+    if (p.precision != DE_PREC_FP64 && p.precision != DE_PREC_MIXED)
+        return set_error(DE_E_INVALID, "precision must be DE_PREC_FP64 or DE_PREC_MIXED (got %d)", p.precision);
     double delta = p.autodelta ? p.radius / p.n : p.delta;  // INIT_STRUCTS input.F90:384
     if (!(delta > 0.0)) return set_error(DE_E_INVALID, "grid spacing must be positive");
     const int nbig_alloc = nn;  // PARAMS%NBIG = 2N+1 (initmod.F90:39)
@@ -259,22 +319,41 @@ DE_API int de_problem_create(const de_params *pin, de_problem **out)
     auto tinv = cached_tinv(nbig_alloc, nbig_solve, p.nsmall, delta);
     const int nbd = 2 * nbig_alloc + 1;
     double *d_tinv = nullptr;
-    DE_CUDA(cudaMalloc(&d_tinv, tinv->size() * sizeof(double)));
+    DE_CUDA(cudaMallocAsync(&d_tinv, tinv->size() * sizeof(double), h->stream));
     const int64_t w = 2 * nn - 1;
-    DE_CUDA(cudaMalloc(&h->d_t1a, h->m * sizeof(double)));
-    DE_CUDA(cudaMalloc(&h->d_v12, w * w * w * sizeof(double)));
+    DE_CUDA(cudaMallocAsync(&h->d_t1a, h->m * sizeof(double), h->stream));
+    DE_CUDA(cudaMallocAsync(&h->d_v12, w * w * w * sizeof(double), h->stream));
     DE_CUDA(cudaMemcpyAsync(d_tinv, tinv->data(), tinv->size() * sizeof(double), cudaMemcpyHostToDevice,
                             h->stream));
     ce = build_tables_launch(nn, p.n, p.charge, delta, d_tinv, nbd, h->d_t1a, h->d_v12, h->stream);
     if (ce != cudaSuccess) return cuda_error(ce, "build_tables");
     DE_CUDA(cudaStreamSynchronize(h->stream));
-    cudaFree(d_tinv);
+    cudaFreeAsync(d_tinv, h->stream);
     hd.t1a = h->d_t1a;
     hd.v12 = h->d_v12;
+    // FP32 copies of T and of the potential tables for the mixed form
+    for (int d = 0; d < nn; ++d) hd.tf[d] = (float)t[d];
+    DE_CUDA(cudaMallocAsync(&h->d_t1af, h->m * sizeof(float), h->stream));
+    DE_CUDA(cudaMallocAsync(&h->d_v12f, w * w * w * sizeof(float), h->stream));
+    ce = to_f32_launch(h->d_t1a, h->d_t1af, h->m, h->stream);
+    if (ce == cudaSuccess) ce = to_f32_launch(h->d_v12, h->d_v12f, w * w * w, h->stream);
+    if (ce != cudaSuccess) return cuda_error(ce, "FP32 tables");
+    DE_CUDA(cudaStreamSynchronize(h->stream));
+    hd.t1af = h->d_t1af;
+    hd.v12f = h->d_v12f;
 
-    DE_CUDA(cudaMalloc(&h->d_small, 64 * 256 * sizeof(double2)));
+    DE_CUDA(cudaMallocAsync(&h->d_small, 64 * 256 * sizeof(double2), h->stream));
     DE_CUDA(cudaMallocHost(&h->h_small, 64 * 256 * sizeof(double2)));
     *out = h.release();
+    return DE_OK;
+}
+
+DE_API int de_problem_trim(de_problem *h)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    std::lock_guard<std::mutex> lk(h->mu);
+    cudaSetDevice(h->p.device);
+    h->trim();
     return DE_OK;
 }
 
@@ -283,18 +362,19 @@ DE_API int de_problem_destroy(de_problem *h)
     if (!h) return DE_OK;
     cudaSetDevice(h->p.device);
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
-    cudaFree(h->d_t1a);
-    cudaFree(h->d_v12);
-    cudaFree(h->d_x);
-    cudaFree(h->d_y);
-    cudaFree(h->d_small);
-    cudaFree(h->d_work);
-    cudaFreeHost(h->h_small);
+    // everything the handle allocated goes back through its own stream
+    cudaStream_t st = h->own_stream ? h->own_stream : h->stream;
+    if (h->stream && h->stream != st) cudaStreamSynchronize(h->stream);
+    for (void *p : {(void *)h->d_t1a, (void *)h->d_v12, (void *)h->d_t1af, (void *)h->d_v12f, (void *)h->d_x,
+                    (void *)h->d_y, (void *)h->d_small, (void *)h->d_work})
+        if (p) cudaFreeAsync(p, st);
+    for (auto &b : h->cache) cudaFreeAsync(b.p, st);
+    cudaStreamSynchronize(st);
+    if (h->h_small) cudaFreeHost(h->h_small);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     for (auto &r : h->ev_pending)
         for (auto ev : r.e) cudaEventDestroy(ev);
     for (auto ev : h->ev_free) cudaEventDestroy(ev);
-    for (auto &b : h->cache) cudaFree(b.p);
     delete h;
     return DE_OK;
 }
@@ -327,12 +407,26 @@ DE_API int de_profile_read(de_problem *h, double *pass_a_ms, double *pass_b_ms, 
     if (!h) return set_error(DE_E_INVALID, "null handle");
     cudaSetDevice(h->p.device);
     DE_TRY(h->harvest());
-    if (pass_a_ms) *pass_a_ms = h->prof_ms[0];
-    if (pass_b_ms) *pass_b_ms = h->prof_ms[1];
-    if (calls) *calls = h->prof_calls;
-    if (vectors) *vectors = h->prof_vectors;
-    h->prof_ms[0] = h->prof_ms[1] = 0.0;
-    h->prof_calls = h->prof_vectors = 0;
+    if (pass_a_ms) *pass_a_ms = h->prof_ms[0][0];
+    if (pass_b_ms) *pass_b_ms = h->prof_ms[0][1];
+    if (calls) *calls = h->prof_calls[0];
+    if (vectors) *vectors = h->prof_vectors[0];
+    h->prof_ms[0][0] = h->prof_ms[0][1] = 0.0;
+    h->prof_calls[0] = h->prof_vectors[0] = 0;
+    return DE_OK;
+}
+
+DE_API int de_profile_read32(de_problem *h, double *pass_a_ms, double *pass_b_ms, int64_t *calls, int64_t *vectors)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    cudaSetDevice(h->p.device);
+    DE_TRY(h->harvest());
+    if (pass_a_ms) *pass_a_ms = h->prof_ms[1][0];
+    if (pass_b_ms) *pass_b_ms = h->prof_ms[1][1];
+    if (calls) *calls = h->prof_calls[1];
+    if (vectors) *vectors = h->prof_vectors[1];
+    h->prof_ms[1][0] = h->prof_ms[1][1] = 0.0;
+    h->prof_calls[1] = h->prof_vectors[1] = 0;
     return DE_OK;
 }
 
@@ -353,6 +447,16 @@ DE_API int de_matblock_d(de_problem *h, const de_complex *x, de_complex *ax, int
     if ((const void *)x == (const void *)ax) return set_error(DE_E_INVALID, "x and ax must not alias");
     cudaSetDevice(h->p.device);
     return h->matblock((const double2 *)x, (double2 *)ax, nev);
+}
+
+DE_API int de_matblock32_d(de_problem *h, const void *x, void *ax, int64_t m, int64_t mb, int nev)
+{
+    if (!h || !x || !ax) return set_error(DE_E_INVALID, "null argument");
+    if (nev < 1) return set_error(DE_E_INVALID, "nev must be >= 1");
+    if (m * mb != h->dim) return set_error(DE_E_SIZE, "SIZE ERRORRRR 66: %lld != %lld", (long long)(m * mb), (long long)h->dim);
+    if (x == (const void *)ax) return set_error(DE_E_INVALID, "x and ax must not alias");
+    cudaSetDevice(h->p.device);
+    return h->matblock32((const float2 *)x, (float2 *)ax, nev);
 }
 
 DE_API int de_matblock(de_problem *h, const de_complex *x, de_complex *ax, int64_t m, int64_t mb, int nev)

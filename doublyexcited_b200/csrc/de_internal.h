@@ -72,6 +72,7 @@ struct de_problem {
     double delta = 0.0;
     de::HamDev ham{};
     double *d_t1a = nullptr, *d_v12 = nullptr;
+    float *d_t1af = nullptr, *d_v12f = nullptr;  // FP32 copies (mixed form)
     cudaStream_t own_stream = nullptr, stream = nullptr;
     // staging buffers for host-pointer calls
     double2 *d_x = nullptr, *d_y = nullptr;
@@ -88,10 +89,14 @@ struct de_problem {
     struct Rec {
         cudaEvent_t e[3];
         int nvec;
+        int f32;  // an FP32 (mixed-form) matvec
     };
     std::vector<Rec> ev_pending;
-    double prof_ms[2] = {0.0, 0.0};
-    int64_t prof_calls = 0, prof_vectors = 0;
+    double prof_ms[2][2] = {{0.0, 0.0}, {0.0, 0.0}};  // [fp64/fp32][pass]
+    int64_t prof_calls[2] = {0, 0}, prof_vectors[2] = {0, 0};
+    int prof_begin(Rec &r);
+    int prof_mid(Rec &r);
+    int prof_end(Rec &r);
     int harvest();
     cudaEvent_t take_event();
 
@@ -104,9 +109,13 @@ struct de_problem {
     std::vector<Blk> cache;
     void *cache_get(size_t bytes);
     void cache_put(void *p);
+    void trim();                   // release idle cached blocks and staging
+    int64_t cached_bytes() const;  // device bytes the handle holds beyond its tables
 
     int ensure_stage(int64_t elems);
     int ensure_work(int64_t elems);
     // device pointers; y = (H + shift) x
     int matblock(const double2 *x, double2 *y, int nvec, double2 shift = double2{0.0, 0.0});
+    // the same in FP32 on complex64 vectors (the mixed form's inner solve)
+    int matblock32(const float2 *x, float2 *y, int nvec, double2 shift = double2{0.0, 0.0});
 };

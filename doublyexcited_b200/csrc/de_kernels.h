@@ -26,6 +26,10 @@ struct HamDev {
     double sre, sim;        // SCALE = exp(i theta) (initmod.F90:48)
     const double *t1a;      // [M]  A*TINV(r_p), A = -Z/delta^3 (hammod.F90:576-577)
     const double *v12;      // [(2NN-1)^3] TINV(r_q - r_p)/delta^3 (hammod.F90:578)
+    // FP32 copies for the mixed form (null when the problem is FP64 only)
+    float tf[kMaxNN];
+    const float *t1af;
+    const float *v12f;
 };
 
 // Y(:,:,v) = H X(:,:,v) for v < nvec; vectors are vstride elements apart.
@@ -39,18 +43,26 @@ cudaError_t hammult_launch(const HamDev &h, const double2 *x, double2 *y, int nv
 // electron-1 (Y += ...).
 cudaError_t hammult_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec,
                                 int64_t vstride, int pass, cudaStream_t st, double2 shift = double2{0.0, 0.0});
+// The same on complex64 vectors in FP32 arithmetic (needs h.tf / t1af / v12f).
+cudaError_t hammult_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride, int pass,
+                                cudaStream_t st, double2 shift = double2{0.0, 0.0});
 
 // One-electron H (NELEC=1): KEMULT1 + V (hammod.F90:71-134).
 cudaError_t hammult1_launch(const HamDev &h, const double *vfull, const double2 *x, double2 *y,
                             int nvec, int64_t vstride, cudaStream_t st);
 
-// Column list: column c is a[c] - sigma * b[c] (b[c] may be null).
-struct ColList {
-    const double2 *a[kMaxCols];
-    const double2 *b[kMaxCols];
+// Column list: column c is a[c] - sigma * b[c] (b[c] may be null).  S is
+// the storage type (double2, or float2 for the mixed form's inner solve);
+// sums accumulate in FP64 either way.
+template <class S>
+struct ColListT {
+    const S *a[kMaxCols];
+    const S *b[kMaxCols];
     double2 sigma;
     int n;
 };
+using ColList = ColListT<double2>;
+using ColListF = ColListT<float2>;
 
 // G(i,j) = sum_r op(L_i[r]) R_j[r] over len rows; op = conj (herm=1) or
 // identity (herm=0).  out is device memory, column-major with leading
@@ -58,18 +70,26 @@ struct ColList {
 int64_t gram_work_elems(int nl, int nr, int64_t len);
 cudaError_t gram_launch(const ColList &L, const ColList &R, int64_t len, int herm, double2 *out,
                         int ldo, double2 *work, cudaStream_t st);
+cudaError_t gram_launch(const ColListF &L, const ColListF &R, int64_t len, int herm, double2 *out, int ldo,
+                        double2 *work, cudaStream_t st);
 
 // Y_j = beta_j * Y_j + alpha * sum_i X_i C(i,j) for j < nout (nout <= 16,
 // nin <= kMaxCols); C is DEVICE memory (complex, column-major, ldc).  Each
 // row is read before it is written, so Y may alias X columns.
-struct UpdList {
-    const double2 *x[kMaxCols];
-    double2 *y[16];
+template <class SI, class SO>
+struct UpdListT {
+    const SI *x[kMaxCols];
+    SO *y[16];
     double2 beta[16];
     double2 alpha;  // Y_j = beta_j Y_j + alpha * sum_i X_i C(i,j)
     int nin, nout;
 };
+using UpdList = UpdListT<double2, double2>;
 cudaError_t update_launch(const UpdList &U, const double2 *c_dev, int ldc, int64_t len,
+                          cudaStream_t st);
+cudaError_t update_launch(const UpdListT<float2, float2> &U, const double2 *c_dev, int ldc, int64_t len,
+                          cudaStream_t st);
+cudaError_t update_launch(const UpdListT<float2, double2> &U, const double2 *c_dev, int ldc, int64_t len,
                           cudaStream_t st);
 
 // out_j = a_j + s * c_j * b_j, c_j from DEVICE memory (j < n, n <= 64).
@@ -87,6 +107,8 @@ cudaError_t dotdiag_launch(const double2 *const *a, const double2 *const *b, int
 // factor is also left in cout[0].  work as for gram (ticket at work[0]).
 cudaError_t gs_update_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
                              const double2 *d, int64_t len, double2 *work, double2 *cout, cudaStream_t st);
+cudaError_t gs_update_launch(const float2 *const *qp, const float2 *const *vp, int m, float2 *q, float2 *v,
+                             const double2 *d, int64_t len, double2 *work, double2 *cout, cudaStream_t st);
 
 // First pass of the fused two-pass Gram-Schmidt (m <= 16): q -= qp d,
 // v -= vp d with pass-1 coefficients d, and the pass-2 coefficients
@@ -94,18 +116,27 @@ cudaError_t gs_update_launch(const double2 *const *qp, const double2 *const *vp,
 // is gs_pass2_launch with d2 = dout.
 cudaError_t gs_pass1_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
                             const double2 *d, int64_t len, double2 *work, double2 *dout, cudaStream_t st);
+cudaError_t gs_pass1_launch(const float2 *const *qp, const float2 *const *vp, int m, float2 *q, float2 *v,
+                            const double2 *d, int64_t len, double2 *work, double2 *dout, cudaStream_t st);
 
 // Second pass: q <- (q - qp d2)/|w|, v <- (v - vp d2)/|w| with
 // |w|^2 = d2[64] - |d2[0..m)|^2; the factor also goes to cout[0].
 cudaError_t gs_pass2_launch(const double2 *const *qp, const double2 *const *vp, int m, double2 *q, double2 *v,
                             const double2 *d2, int64_t len, double2 *cout, cudaStream_t st);
+cudaError_t gs_pass2_launch(const float2 *const *qp, const float2 *const *vp, int m, float2 *q, float2 *v,
+                            const double2 *d2, int64_t len, double2 *cout, cudaStream_t st);
+
+// Narrowing copies to FP32 (complex and real).
+cudaError_t to_f32_launch(const double2 *x, float2 *y, int64_t n, cudaStream_t st);
+cudaError_t to_f32_launch(const double *x, float *y, int64_t n, cudaStream_t st);
 
 // k x k (k <= 16) dense helpers that keep the solver on the device.
 // flag bits: 1 Cholesky breakdown, 2 all-zero block, 4 orthonormality
 // self-check failed, 8 singular 1 x 1 Gram.
 cudaError_t small_cholinv_launch(const double2 *g, int k, double2 *rinv, int *flag, cudaStream_t st);
 cudaError_t small_hsqrt1_launch(const double2 *g, double2 *ginvh, double2 *gsq, int *flag, cudaStream_t st);
-cudaError_t small_ortho_check_launch(const double2 *t, int k, int *flag, cudaStream_t st);
+// |T - I| <= tol elementwise (the reference's self-check uses 1e-10).
+cudaError_t small_ortho_check_launch(const double2 *t, int k, int *flag, cudaStream_t st, double tol = 1e-10);
 cudaError_t small_gemm_launch(const double2 *a, const double2 *b, double2 *c, int m, int k, int n, cudaStream_t st);
 
 // x_j *= c_j (c from DEVICE, complex), in place.

@@ -21,7 +21,18 @@
 //    (harmonic_ritz_small.F90:145-156) never reach the solution and are not
 //    formed; only the first block column of lanham is (rhs is zero below it,
 //    :309-316).
+//
+// Mixed precision (de_params.precision = DE_PREC_MIXED): the inner solve of
+// PRECBLOCK_BASIC - a fixed-order approximation of (H - sigma)^-1 used only
+// as a preconditioner - keeps its Krylov blocks in complex64 and runs its
+// matvecs in FP32 arithmetic, with FP64 sums in every reduction.  The outer
+// iteration (cholQR, the harmonic projection and its generalized
+// eigenproblem, the residual norms and every MATBLOCK) stays FP64, so each
+// outer step is an FP64-residual refinement of the Ritz pairs and the
+// converged eigenvalues meet the FP64 tolerance.  The inner solve's
+// orthonormality self-check is held to 1e-5 instead of 1e-10 there.
 #include <algorithm>
+#include <type_traits>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -52,10 +63,12 @@ struct Solver {
     double2 *X = nullptr, *AX = nullptr, *W = nullptr, *AW = nullptr;
     double2 *S = nullptr, *AS = nullptr, *P = nullptr, *AP = nullptr;
     double2 *LV = nullptr, *LQ = nullptr;  // inner solve: order*nev each
+    float2 *LV32 = nullptr, *LQ32 = nullptr;  // the same in complex64 (mixed)
+    bool mixed = false;
     double2 *dG = nullptr, *dC = nullptr, *dE = nullptr, *dR = nullptr, *dT = nullptr, *dT2 = nullptr;
     double2 *dRinv = nullptr, *dGinvh = nullptr, *dGsq = nullptr, *dG1 = nullptr, *dSV = nullptr;
     int *dFlags = nullptr;
-    double2 *hbuf = nullptr;  // pinned 64 x 128
+    double2 *hbuf = nullptr;  // pinned staging for k x k results (>= 64 x 128 + 64)
     std::vector<double2 *> allocs;
 
     int64_t mv_exec = 0, mv_ref = 0;
@@ -64,7 +77,6 @@ struct Solver {
     ~Solver()
     {
         for (auto p : allocs) h->cache_put(p);
-        if (hbuf) cudaFreeHost(hbuf);
     }
 
     double2 *col(double2 *b, int j) const { return b + (int64_t)j * D; }
@@ -89,8 +101,14 @@ struct Solver {
             DE_TRY(alloc(&AS, D * ldr));
         }
         if (order > 0) {
-            DE_TRY(alloc(&LV, D * (int64_t)std::max(1, order) * nev));
-            DE_TRY(alloc(&LQ, D * (int64_t)std::max(1, order) * nev));
+            const int64_t n = D * (int64_t)std::max(1, order) * nev;
+            if (mixed && order > 1) {  // complex64: half the bytes
+                DE_TRY(alloc(reinterpret_cast<double2 **>(&LV32), (n + 1) / 2));
+                DE_TRY(alloc(reinterpret_cast<double2 **>(&LQ32), (n + 1) / 2));
+            } else {
+                DE_TRY(alloc(&LV, n));
+                DE_TRY(alloc(&LQ, n));
+            }
         }
         DE_TRY(alloc(&dG, 64 * 128));
         DE_TRY(alloc(&dC, 128 * 16));
@@ -109,7 +127,7 @@ struct Solver {
             dFlags = reinterpret_cast<int *>(f);
             DE_CUDA(cudaMemsetAsync(dFlags, 0, 4 * sizeof(double2), st));
         }
-        DE_CUDA(cudaMallocHost(&hbuf, (64 * 128 + 64) * sizeof(double2)));
+        hbuf = h->h_small;  // pinned, 64 x 256 (the handle is locked for the solve)
         const int64_t wk = std::max<int64_t>(gram_work_elems(64, 128, D), dotdiag_work_elems(64, D));
         DE_TRY(h->ensure_work(wk));
         return DE_OK;
@@ -312,12 +330,102 @@ struct Solver {
     }
 
     // ---- inner solve -------------------------------------------------------
+    // Storage-generic pieces: S = double2 (plain FP64) or float2 (mixed).
+    template <class S>
+    S *lv_buf()
+    {
+        if constexpr (std::is_same_v<S, double2>) return LV;
+        else return LV32;
+    }
+    template <class S>
+    S *lq_buf()
+    {
+        if constexpr (std::is_same_v<S, double2>) return LQ;
+        else return LQ32;
+    }
+    template <class S>
+    static ColListT<S> colsT(S *base, int k, int64_t D)
+    {
+        ColListT<S> L{};
+        L.n = k;
+        for (int j = 0; j < k; ++j) L.a[j] = base + (int64_t)j * D;
+        return L;
+    }
+    template <class S>
+    int gramT(const ColListT<S> &L, const ColListT<S> &R, double2 *out, int ldo)
+    {
+        cudaError_t e = gram_launch(L, R, D, 1, out, ldo, h->d_work, st);
+        if (e != cudaSuccess) return cuda_error(e, "gram");
+        return DE_OK;
+    }
+    template <class S>
+    int gram_hostT(const ColListT<S> &L, const ColListT<S> &R, std::vector<cplx> &g)
+    {
+        DE_TRY(gramT(L, R, dG, L.n));
+        DE_CUDA(cudaMemcpyAsync(hbuf, dG, (size_t)L.n * R.n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        int *hf = reinterpret_cast<int *>(hbuf + (size_t)L.n * R.n);
+        DE_CUDA(cudaMemcpyAsync(hf, dFlags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        DE_CUDA(cudaStreamSynchronize(st));
+        DE_TRY(check_flags(hf[1]));
+        g.resize((size_t)L.n * R.n);
+        for (size_t i = 0; i < g.size(); ++i) g[i] = cplx(hbuf[i].x, hbuf[i].y);
+        return DE_OK;
+    }
+    // Y[0..nout) = sum_i X_i C(i, j), X: nin columns from xb, Y columns from yb
+    template <class SI, class SO>
+    int updateT(const SI *xb, int nin, SO *yb, int nout, const double2 *c, int ldc)
+    {
+        UpdListT<SI, SO> U{};
+        U.nin = nin;
+        U.nout = nout;
+        if (nin > kMaxCols || nout > 16) return set_error(DE_E_INVALID, "update too wide");
+        for (int i = 0; i < nin; ++i) U.x[i] = xb + (int64_t)i * D;
+        for (int j = 0; j < nout; ++j) {
+            U.y[j] = yb + (int64_t)j * D;
+            U.beta[j] = make_double2(0.0, 0.0);
+        }
+        U.alpha = make_double2(1.0, 0.0);
+        cudaError_t e = update_launch(U, c, ldc, D, st);
+        if (e != cudaSuccess) return cuda_error(e, "update");
+        return DE_OK;
+    }
+    // H x (the inner solve's callback) and (H - sigma) x
+    template <class S>
+    int mult_plain(const S *x, S *y, int k)
+    {
+        if constexpr (std::is_same_v<S, double2>) {
+            return inner_mult(x, y, k);
+        } else {
+            mv_exec += k;
+            mv_ref += k;
+            return h->matblock32(x, y, k);
+        }
+    }
+    template <class S>
+    int mult_shifted(const S *x, S *y, int k)
+    {
+        if constexpr (std::is_same_v<S, double2>) {
+            return inner_mult_shifted(x, y, k);
+        } else {
+            mv_exec += k;
+            mv_ref += k;
+            const cplx ms = -sigma;
+            return h->matblock32(x, y, k, make_double2(ms.real(), ms.imag()));
+        }
+    }
+
     // myhgramschmidt_many with factors (1,0): two classical passes of the
     // (H-sigma)-weighted Gram-Schmidt of the pair (q, v) against the first m
     // pairs of (LQ, LV).
-    int hgram(int m, double2 *q, double2 *v)
+    template <class S>
+    int hgram(int m, S *q, S *v)
     {
-        std::vector<const double2 *> qp = cl(LQ, m), vp = cl(LV, m);
+        S *LQs = lq_buf<S>(), *LVs = lv_buf<S>();
+        std::vector<const S *> qp(m), vp(m);
+        for (int i = 0; i < m; ++i) {
+            qp[i] = LQs + (int64_t)i * D;
+            vp[i] = LVs + (int64_t)i * D;
+        }
         cudaError_t e;
         if (m == 0) {  // nothing to project: the two passes only normalise
             e = gs_update_launch(qp.data(), vp.data(), 0, q, v, dT, D, h->d_work, dR, st);
@@ -327,7 +435,7 @@ struct Solver {
         if (m <= 16) {
             // pass 1 with the pass-2 coefficients fused into its update; the
             // intermediate normalisation of the reference cancels exactly.
-            DE_TRY(gram_dev(cols(LQ, m, D), cols(q, 1, D), dT, m));
+            DE_TRY(gramT(colsT(LQs, m, D), colsT(q, 1, D), dT, m));
             e = gs_pass1_launch(qp.data(), vp.data(), m, q, v, dT, D, h->d_work, dT2, st);
             if (e != cudaSuccess) return cuda_error(e, "gs_pass1");
             e = gs_pass2_launch(qp.data(), vp.data(), m, q, v, dT2, D, dR, st);
@@ -335,15 +443,13 @@ struct Solver {
             return DE_OK;
         }
         for (int pass = 0; pass < 2; ++pass) {
-            DE_TRY(gram_dev(cols(LQ, m, D), cols(q, 1, D), dT, m));
+            DE_TRY(gramT(colsT(LQs, m, D), colsT(q, 1, D), dT, m));
             e = gs_update_launch(qp.data(), vp.data(), m, q, v, dT, D, h->d_work, dR, st);
             if (e != cudaSuccess) return cuda_error(e, "gs_update");
         }
         return DE_OK;
     }
 
-    // basicblocklansolve harmonic_ritz_small.F90:258-324 on block b (k
-    // columns), in place: b <- V (Q^H V_1) G^{1/2}.
     int shift_sub(double2 *q, const double2 *v, int k)  // q <- q - sigma v
     {
         const cplx ms = -sigma;
@@ -354,20 +460,31 @@ struct Solver {
         return DE_OK;
     }
 
+    // basicblocklansolve harmonic_ritz_small.F90:258-324 on block b (k
+    // columns), in place: b <- V (Q^H V_1) G^{1/2}.  S is the storage of
+    // the Krylov blocks; b is always FP64.
+    template <class S>
     int basic(double2 *b, int k)
     {
+        S *V = lv_buf<S>(), *Q = lq_buf<S>();
+        const double ortho_tol = std::is_same_v<S, double2> ? 1e-10 : 1e-5;
         // harm_orthog_oneblock :161-244
-        DE_CUDA(cudaMemcpyAsync(LV, b, (size_t)k * D * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-        DE_TRY(inner_mult_shifted(LV, LQ, k));
+        if constexpr (std::is_same_v<S, double2>) {
+            DE_CUDA(cudaMemcpyAsync(V, b, (size_t)k * D * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+        } else {
+            cudaError_t e = to_f32_launch(b, V, (int64_t)k * D, st);
+            if (e != cudaSuccess) return cuda_error(e, "to_f32");
+        }
+        DE_TRY(mult_shifted(V, Q, k));
         std::vector<cplx> gsq;
         if (k == 1) {  // 1 x 1 Gram: its square roots on the device
-            DE_TRY(gram_dev(cols(LQ, 1, D), cols(LQ, 1, D), dG, 1));
+            DE_TRY(gramT(colsT(Q, 1, D), colsT(Q, 1, D), dG, 1));
             cudaError_t e = small_hsqrt1_launch(dG, dGinvh, dGsq, dFlags, st);
             if (e != cudaSuccess) return cuda_error(e, "small_hsqrt1");
-            DE_TRY(update(cl(LV, 1), clw(LV, 1), dGinvh, 1, 1.0, 0.0));
+            DE_TRY(updateT(V, 1, V, 1, dGinvh, 1));
         } else {
             std::vector<cplx> g, ginv;
-            DE_TRY(gram_host(cols(LQ, k, D), cols(LQ, k, D), g));
+            DE_TRY(gram_hostT(colsT(Q, k, D), colsT(Q, k, D), g));
             auto t0 = clk::now();
             DE_TRY(herm_sqrt_pair(k, g, ginv, gsq));
             t_dense += secs(t0, clk::now());
@@ -375,36 +492,36 @@ struct Solver {
             for (int j = 0; j < k; ++j)
                 for (int i = 0; i < k; ++i) ginvh[i + (size_t)k * j] = std::conj(ginv[j + (size_t)k * i]);
             DE_TRY(upload(ginvh, dC));
-            DE_TRY(update(cl(LV, k), clw(LV, k), dC, k, 1.0, 0.0));
+            DE_TRY(updateT(V, k, V, k, dC, k));
         }
-        // self-check: (H - sigma) V_1 orthonormal to 1e-10
-        DE_TRY(inner_mult_shifted(LV, LQ, k));
-        DE_TRY(gram_dev(cols(LQ, k, D), cols(LQ, k, D), dT, k));
+        // self-check: (H - sigma) V_1 orthonormal
+        DE_TRY(mult_shifted(V, Q, k));
+        DE_TRY(gramT(colsT(Q, k, D), colsT(Q, k, D), dT, k));
         {
-            cudaError_t e = small_ortho_check_launch(dT, k, dFlags, st);
+            cudaError_t e = small_ortho_check_launch(dT, k, dFlags, st, ortho_tol);
             if (e != cudaSuccess) return cuda_error(e, "small_ortho_check");
         }
         // fast_harmritz_setup :86-158 (maxiter = M^2 never truncates a block)
         for (int io = 0; io < order; ++io) {
-            double2 *vb = col(LV, io * k), *qb = col(LQ, io * k);
+            S *vb = V + (int64_t)io * k * D, *qb = Q + (int64_t)io * k * D;
             if (io > 0) {
-                DE_TRY(inner_mult(col(LV, (io - 1) * k), vb, k));
-                DE_TRY(inner_mult_shifted(vb, qb, k));
+                DE_TRY(mult_plain(V + (int64_t)(io - 1) * k * D, vb, k));
+                DE_TRY(mult_shifted(vb, qb, k));
             } else {
                 mv_ref += compat ? 1 : k;  // the reference recomputes the product checked above
             }
-            for (int i = 0; i < k; ++i) DE_TRY(hgram(io * k + i, col(qb, i), col(vb, i)));
+            for (int i = 0; i < k; ++i) DE_TRY(hgram(io * k + i, qb + (int64_t)i * D, vb + (int64_t)i * D));
         }
         // solution: V (lanham rhs), rhs(:,1,:) = G^{1/2} (:309-316)
         const int thisdim = order * k;
         if (k == 1) {
-            DE_TRY(gram_dev(cols(LQ, thisdim, D), cols(LV, 1, D), dG1, thisdim));
+            DE_TRY(gramT(colsT(Q, thisdim, D), colsT(V, 1, D), dG1, thisdim));
             cudaError_t e = small_gemm_launch(dG1, dGsq, dSV, thisdim, 1, 1, st);
             if (e != cudaSuccess) return cuda_error(e, "small_gemm");
-            return update(cl(LV, thisdim), clw(b, 1), dSV, thisdim, 1.0, 0.0);
+            return updateT(V, thisdim, b, 1, dSV, thisdim);
         }
         std::vector<cplx> g1;  // Q^H V_1, thisdim x k (first block column of lanham)
-        DE_TRY(gram_host(cols(LQ, thisdim, D), cols(LV, k, D), g1));
+        DE_TRY(gram_hostT(colsT(Q, thisdim, D), colsT(V, k, D), g1));
         std::vector<cplx> sv((size_t)thisdim * k, 0.0);
         for (int j = 0; j < k; ++j)
             for (int i = 0; i < thisdim; ++i) {
@@ -413,7 +530,7 @@ struct Solver {
                 sv[i + (size_t)thisdim * j] = s;
             }
         DE_TRY(upload(sv, dC));
-        return update(cl(LV, thisdim), clw(b, k), dC, thisdim, 1.0, 0.0);
+        return updateT(V, thisdim, b, k, dC, thisdim);
     }
 
     // PRECBLOCK gplmr.F90:466-502 (in place)
@@ -429,8 +546,10 @@ struct Solver {
             }
         } else if (gm.usepetscflag == 0) {
             s = set_error(DE_E_UNSUPPORTED, "usepetscflag=0 selects the PETSc KSP inner solve, which this build does not provide");
+        } else if (mixed) {
+            s = basic<float2>(b, k);
         } else {
-            s = basic(b, k);
+            s = basic<double2>(b, k);
         }
         t_prec += secs(t0, clk::now());
         return s;
@@ -640,6 +759,9 @@ DE_API int de_gplmr_eig_d(de_problem *h, de_complex *x_d, de_complex *e, int64_t
     s.gm = g;
     s.order = g.max_inner_iter;
     s.compat = g.compat_first_column_only != 0;
+    s.mixed = h->p.precision == DE_PREC_MIXED;
+    if (s.mixed && s.compat)
+        return set_error(DE_E_UNSUPPORTED, "the first-column-only mode is kept for the FP64 form only");
     s.sigma = cplx(sigma.re, sigma.im);
     if (stats) std::memset(stats, 0, sizeof *stats);
     return s.run((double2 *)x_d, e, maxit, tol, outmodulus, stats);
@@ -653,7 +775,7 @@ DE_API int de_gplmr_eig(de_problem *h, de_complex *x, de_complex *e, int64_t m, 
     cudaSetDevice(h->p.device);
     double2 *xd = nullptr;
     const size_t bytes = (size_t)h->dim * nev * sizeof(double2);
-    DE_CUDA(cudaMalloc(&xd, bytes));
+    DE_CUDA(cudaMallocAsync(&xd, bytes, h->stream));
     int s = DE_OK;
     cudaError_t ce = cudaMemcpyAsync(xd, x, bytes, cudaMemcpyHostToDevice, h->stream);
     if (ce != cudaSuccess) s = cuda_error(ce, "H2D");
@@ -663,7 +785,8 @@ DE_API int de_gplmr_eig(de_problem *h, de_complex *x, de_complex *e, int64_t m, 
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
         if (ce != cudaSuccess) s = cuda_error(ce, "D2H");
     }
-    cudaFree(xd);
+    cudaFreeAsync(xd, h->stream);
+    if (s != DE_OK) cudaStreamSynchronize(h->stream);
     return s;
 }
 

@@ -123,6 +123,11 @@ DE_API void de_params_default(de_params *p);
  * POTENTIAL1/2 hammod.F90:432-582).  Allocates device tables only. */
 DE_API int de_problem_create(const de_params *p, de_problem **out);
 DE_API int de_problem_destroy(de_problem *h);
+/* Release the device workspace a handle keeps between solves (GPLMR blocks,
+ * staging) back to the stream-ordered pool; the operator tables stay.  The
+ * reference keeps SAVE'd work arrays for the life of the process
+ * (hammod.F90:153-159); this is the way to give them back. */
+DE_API int de_problem_trim(de_problem *h);
 
 /* NN, M = NN^3 and the vector length M^nelec of a handle. */
 DE_API int de_problem_dims(const de_problem *h, int *nn, int64_t *m, int64_t *dim);
@@ -141,6 +146,10 @@ DE_API int de_set_profiling(de_problem *h, int on);
  * multiplied since the last read (waits for the recorded events); resets. */
 DE_API int de_profile_read(de_problem *h, double *pass_a_ms, double *pass_b_ms, int64_t *calls,
                            int64_t *vectors);
+/* The same for the FP32 matvecs of the mixed form's inner solve (no
+ * counterpart in the reference, which has one precision). */
+DE_API int de_profile_read32(de_problem *h, double *pass_a_ms, double *pass_b_ms, int64_t *calls,
+                             int64_t *vectors);
 
 /* ---- operator: HAMMULT / MATBLOCK / MYMATMUL ------------------------- */
 
@@ -156,6 +165,11 @@ DE_API int de_matblock(de_problem *h, const de_complex *x, de_complex *ax, int64
                        int nev);
 DE_API int de_matblock_d(de_problem *h, const de_complex *x_d, de_complex *ax_d, int64_t m,
                          int64_t mb, int nev);
+/* MATBLOCK in the mixed form's precision: complex64 device vectors
+ * ({float re, im} interleaved, same layout), FP32 arithmetic.  No
+ * counterpart in the reference (one precision there); it is the inner-solve
+ * matvec of DE_PREC_MIXED, exported for accuracy and throughput checks. */
+DE_API int de_matblock32_d(de_problem *h, const void *x_d, void *ax_d, int64_t m, int64_t mb, int nev);
 
 /* OUT(i,j) = <BRA_i, KET_j> over vectors of length size.  hermitian=1:
  * conj(BRA).KET (MYDOTSUB doublyexcited.F90:47-59, MPIHERMDOT
@@ -248,6 +262,63 @@ DE_API int de_read_vectors(const char *path, int64_t m, int num, de_complex *psi
 
 /* Header of an eigenvector file: its M and number of vectors. */
 DE_API int de_vectors_header(const char *path, int64_t *m, int *num);
+
+/* ---- batched and served solves ----------------------------------------
+ * No counterpart in the reference, which runs one GPLMR_EIG per MPI job
+ * (doublyexcited.F90:238-241); these entry points run many independent
+ * GPLMR_EIG solves of uneven size on one GPU at once.
+ *
+ * A server owns `workers` host threads, each with its own CUDA stream and
+ * handles, so the kernels of different solves overlap on the device.
+ * Requests are admitted in arrival order (first come, first served; the
+ * head of the queue waits rather than being overtaken) when a worker is
+ * free and the request's device footprint fits in what is left of
+ * `max_bytes`; a request whose footprint alone exceeds max_bytes is
+ * refused at submission with DE_E_BUSY.  A request's Krylov blocks stay on
+ * the device for the whole solve; its host buffers x and e must stay valid
+ * until its result has been collected. */
+typedef struct {
+    int device;        /* CUDA device ordinal */
+    int workers;       /* concurrent solves (streams), >= 1 */
+    int64_t max_bytes; /* device bytes for admitted solves; 0 = 90% of the free memory at creation */
+} de_server_opts;
+
+typedef struct {
+    de_params params;   /* operator and precision of this solve (params.device is ignored) */
+    de_complex sigma;   /* GPLMR shift */
+    int nev, ns, maxit;
+    double tol;
+    de_gmres gm;
+    de_complex *x;      /* host, M^2 x NEV column-major: start vectors in, Ritz vectors out */
+    de_complex *e;      /* host, NEV eigenvalues out */
+} de_request;
+
+typedef struct {
+    uint64_t id;
+    int status;                     /* DE_OK or the solve's error */
+    de_stats stats;
+    double t_submit_s, t_start_s, t_end_s;  /* server clock, seconds since creation */
+    int64_t footprint_bytes;        /* device bytes reserved for the solve */
+    int worker;
+} de_result;
+
+/* Device bytes a request reserves: the GPLMR blocks (X AX W AW P AP, S AS,
+ * the inner solve's Krylov blocks, complex64 in the mixed form), staging
+ * and the operator tables. */
+DE_API int de_request_footprint(const de_request *r, int64_t *bytes);
+DE_API int de_server_create(const de_server_opts *o, void **server);
+/* Queue a request; its id is returned in *id. */
+DE_API int de_server_submit(void *server, const de_request *r, uint64_t *id);
+/* Wait for request id (timeout_s < 0: no limit); DE_E_BUSY on timeout. */
+DE_API int de_server_wait(void *server, uint64_t id, double timeout_s, de_result *out);
+/* Wait for any finished request not yet collected. */
+DE_API int de_server_wait_any(void *server, double timeout_s, de_result *out);
+/* Seconds on the server clock. */
+DE_API double de_server_now(void *server);
+/* Requests queued, running, and device bytes reserved right now. */
+DE_API int de_server_load(void *server, int *queued, int *running, int64_t *bytes_reserved);
+/* Finishes the running solves, drops the queued ones, frees everything. */
+DE_API int de_server_destroy(void *server);
 
 #ifdef __cplusplus
 }

@@ -167,3 +167,27 @@ def test_invalid_params_rejected(de):
     with pytest.raises(de.DeError) as e:
         de.Problem(n=2, nelec=3)
     assert e.value.status == de.DE_E_INVALID
+
+
+def test_request_footprint_counts_the_solver_blocks(de):
+    """Admission arithmetic of the server (host only): complex128 GPLMR blocks
+    X AX W AW P AP S AS, the inner solve's Krylov blocks (complex64 in the
+    mixed form), reduction scratch and operator tables."""
+    x = np.zeros((7 ** 6, 2), np.complex128, order="F")
+    req = de.Server.request(3, x, -0.78, ns=5, max_inner_iter=5)
+    d, nev, ns, order = 7 ** 6, 2, 5, 5
+    blocks = (6 * nev + 2 * ns * nev) * d * 16
+    fp64 = de.Server.footprint(req)
+    assert blocks + 2 * order * nev * d * 16 < fp64 < blocks + 2 * order * nev * d * 16 + (64 << 20)
+    req_m = de.Server.request(3, x, -0.78, ns=5, max_inner_iter=5, precision="mixed")
+    assert fp64 - de.Server.footprint(req_m) == order * nev * d * 16
+
+
+def test_server_create_fails_loudly_without_gpu(de):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(de.DeError) as e:
+        de.Server(workers=2)
+    assert e.value.status == de.DE_E_CUDA

@@ -108,6 +108,30 @@ def test_device_pointer_api(de, oracle):
     assert np.array_equal(y, ref)
 
 
+@pytest.mark.parametrize("n,theta", [(3, 0.2), (5, 0.35), (6, 0.2)])
+def test_fp32_matvec_relative_error(de, oracle, n, theta):
+    """The mixed form's FP32 matvec on complex64 inputs, per call, against
+    the FP64 oracle's H x: relative 2-norm error within 1e-6 (FP32 unit
+    roundoff 6e-8 times the contraction length and the conditioning of T).
+    The first column is sampled at N=6 to keep the oracle fast."""
+    import torch
+
+    p = oracle.Params(n=n, delta=2.0, theta=theta)
+    h = oracle.init_hamiltonian(p, nelec=2)
+    x = oracle.seeded_vectors(p.m ** 2, 2, 21)
+    x32 = x.astype(np.complex64)
+    with de.Problem(n=n, delta=2.0, theta=theta, precision="mixed") as g:
+        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        xd = torch.from_numpy(np.ascontiguousarray(x32.T)).cuda()
+        yd = torch.empty_like(xd)
+        g.matblock32_d(xd.data_ptr(), yd.data_ptr(), 2)
+        y = yd.cpu().numpy().T
+    for j in range(2 if n < 6 else 1):
+        ref = h.matvec(x32[:, j].astype(np.complex128))
+        rel = np.linalg.norm(y[:, j] - ref) / np.linalg.norm(ref)
+        assert rel < 1e-6, rel
+
+
 @pytest.mark.parametrize("n", [9, 10])
 def test_full_size_properties(de, n):
     """At the benchmark sizes (N=9: 753 MB per vector) the oracle is too
