@@ -49,6 +49,62 @@ WORKLOADS = {
 }
 
 
+# Served stream: Poisson arrivals of uneven solve requests (seeded); sizes
+# are the batched configuration's mix scaled to grids a few-minute run can
+# finish (N 3-6 instead of 4-8, NEV 1-2 instead of 2-8).
+SERVE = dict(requests=40, rate=40.0, seed=4, ns=[3, 4, 5, 6], n_weights=[0.2, 0.3, 0.3, 0.2],
+             thetas=[0.20, 0.25, 0.30, 0.35, 0.40, 0.45, 0.50], nevs=[1, 1, 1, 2], spins=["singlet", "triplet"],
+             sigma=-0.7131541429, tol=1e-8, maxit=120, workers=4)
+
+
+def serve_requests(cfg):
+    import numpy as np
+
+    rng = np.random.Generator(np.random.PCG64(cfg["seed"]))
+    t = 0.0
+    out = []
+    for k in range(cfg["requests"]):
+        t += rng.exponential(1.0 / cfg["rate"])
+        out.append(dict(t=t, n=int(rng.choice(cfg["ns"], p=cfg["n_weights"])), theta=float(rng.choice(cfg["thetas"])),
+                        nev=int(rng.choice(cfg["nevs"])), spin=str(rng.choice(cfg["spins"])), seed=1000 + k))
+    return out
+
+
+def run_served(de, seeded_start, cfg, precision):
+    """Replay the arrival schedule against a Server; latencies from the
+    server clock (submission to completion)."""
+    import numpy as np
+
+    reqs = serve_requests(cfg)
+    srv = de.Server(workers=cfg["workers"])
+    built = []
+    for r in reqs:
+        m = (2 * r["n"] + 1) ** 3
+        x0 = seeded_start(m, r["nev"], r["seed"], r["spin"])
+        built.append(srv.request(r["n"], x0, cfg["sigma"], theta=r["theta"], precision=precision, ns=5,
+                                 maxit=cfg["maxit"], tol=cfg["tol"]))
+    done = {}
+    t0 = srv.now()
+    k = 0
+    while len(done) < len(reqs):
+        now = srv.now() - t0
+        while k < len(reqs) and reqs[k]["t"] <= now:
+            srv.submit(built[k], tag=k)
+            k += 1
+        nxt = (reqs[k]["t"] - now) if k < len(reqs) else 1.0
+        res = srv.wait_any(max(1e-4, min(nxt, 1.0)))
+        if res is not None:
+            done[res.tag] = res
+    t_end = max(r.t_end_s for r in done.values()) - t0
+    srv.close()
+    lat = np.array([done[i].latency_s for i in range(len(reqs))])
+    ok = [done[i].status == 0 for i in range(len(reqs))]
+    conv = [done[i].converged for i in range(len(reqs))]
+    return {"solves_per_s": len(reqs) / t_end, "wall_s": t_end, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "ok": int(sum(ok)),
+            "converged": int(sum(conv)), "e": {i: done[i].e.copy() for i in range(len(reqs))}}
+
+
 def hammults_per_solve(w, iters):
     """The reference's HAMMULT count (ICALLED) for a solve of `iters`
     iterations: NEV for the start, then per iteration (1+NS) MATBLOCKs of NEV
@@ -221,20 +277,65 @@ def run_reference(a, w):
     return 0
 
 
+def serve_main(a):
+    """--workload serve: the served stream, mixed and FP64 back to back on one
+    GPU, one JSON line.  value = mixed solves/s over the stream."""
+    import numpy as np
+    import torch
+
+    import doublyexcited_b200 as de
+    from doublyexcited_b200.starts import seeded_start
+
+    rank, world, local = dist_setup()
+    if a.impl == "reference" or rank != 0:
+        if a.impl == "reference" and rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving layer "
+                              "(one GPLMR_EIG per MPI job)"}))
+        return 0
+    torch.cuda.set_device(local)
+    cfg = dict(SERVE)
+    sampler = ClockSampler(local)
+    l0 = de.lib().de_kernel_launches()
+    sampler.start()
+    mixed = run_served(de, seeded_start, cfg, "mixed")
+    clocks = sampler.stop()
+    launches = de.lib().de_kernel_launches() - l0
+    fp64 = run_served(de, seeded_start, cfg, "fp64")
+    de_max = max(float(np.max(np.abs(np.sort_complex(mixed["e"][i]) - np.sort_complex(fp64["e"][i]))))
+                 for i in mixed["e"])
+    strip = lambda d: {k: v for k, v in d.items() if k != "e"}  # noqa: E731
+    line = {"metric": "resonance solves/s (served stream)", "value": mixed["solves_per_s"], "unit": "solves/s",
+            "n_gpus": 1, "steps": cfg["requests"], "warmup": 0, "ms_per_step": mixed["wall_s"] / cfg["requests"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inner solve / f64 outer iteration", "data": "synthetic (seeded Poisson arrivals, seeded starts)",
+            "config": {"workload": "serve", **{k: v for k, v in cfg.items()}},
+            "p50_s": mixed["p50_s"], "p99_s": mixed["p99_s"], "mixed": strip(mixed), "fp64": strip(fp64),
+            "speedup_vs_fp64": mixed["solves_per_s"] / fp64["solves_per_s"], "dE_mixed_vs_fp64_max": de_max,
+            "gpu_launches": int(launches), "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="solve-n6", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="solve-n6", choices=sorted(WORKLOADS) + ["serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: FP32 inner solve, FP64 outer iteration (the product form); fp64: plain")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip the plain-FP64 solves timed beside the mixed ones")
+    ap.add_argument("--maxit", type=int, default=None,
+                    help="cap the GPLMR iterations (short runs for kernel profiling; not a bench value)")
     a = ap.parse_args()
-    w = WORKLOADS[a.workload]
+    if a.workload == "serve":
+        return serve_main(a)
+    w = dict(WORKLOADS[a.workload])
+    if a.maxit is not None:
+        w["maxit"] = a.maxit
     if a.impl == "reference":
         return run_reference(a, w)
 

@@ -182,6 +182,7 @@ SIGNATURES = {
     "de_server_load": (INT, [P, ctypes.POINTER(INT), ctypes.POINTER(INT), ctypes.POINTER(I64)]),
     "de_server_destroy": (INT, [P]),
     "de_problem_trim": (INT, [P]),
+    "de_set_matvec_kernel": (INT, [P, INT]),
 }
 
 _LIB = None

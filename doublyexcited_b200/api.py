@@ -99,6 +99,13 @@ class Problem:
         stream)."""
         check(lib().de_set_stream(self._h, ctypes.c_void_p(cuda_stream)), "de_set_stream")
 
+    def set_matvec_kernel(self, kind: str) -> None:
+        """'fma' (default): the CUDA-core kernels; 'tensor': the axis
+        contractions on the FP64 tensor cores where built (NN 9..19)."""
+        if kind not in ("tensor", "fma"):
+            raise ValueError("kind must be 'tensor' or 'fma'")
+        check(lib().de_set_matvec_kernel(self._h, 1 if kind == "tensor" else 0), "de_set_matvec_kernel")
+
     def set_profiling(self, on: bool) -> None:
         check(lib().de_set_profiling(self._h, int(bool(on))), "de_set_profiling")
 
@@ -270,10 +277,13 @@ class Server:
     @staticmethod
     def request(n: int, x0: np.ndarray, sigma: complex, *, theta: float = 0.2, delta: float = 2.0,
                 charge: float = 2.0, precision: str = "fp64", ns: int = 5, maxit: int = 100, tol: float = 1e-7,
-                max_inner_iter: int = 5):
+                max_inner_iter: int = 5, autodelta: bool = False, radius: float = 7.0):
+        """A request's buffers: the operator as :class:`Problem` builds it (the
+        same keyword defaults), GPLMR settings as :meth:`Problem.gplmr_eig`."""
         p = de_params()
         lib().de_params_default(ctypes.byref(p))
         p.n, p.delta, p.theta, p.charge = n, delta, theta, charge
+        p.autodelta, p.radius = int(bool(autodelta)), radius
         p.precision = 1 if precision == "mixed" else 0
         x = np.array(x0, dtype=np.complex128, order="F", copy=True)
         if x.ndim == 1:

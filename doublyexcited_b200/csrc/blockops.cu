@@ -440,35 +440,69 @@ __device__ __forceinline__ void block_sum(double (&re)[N], double (&im)[N], doub
 }
 
 // Final sum of nblk per-block partials part[b*stride + o], o < nout <= 32,
-// by the whole 256-thread block in a fixed order: warp g sums the blocks
-// b = g (mod 8) for every output, then one thread per output adds the 8
-// warp sums.  Eight independent load chains instead of one thread's serial
-// chain over all partials; the result does not depend on block timing.
+// by the whole 256-thread block in a fixed order: with np = nout rounded up
+// to a power of two, thread t sums output t % np over the blocks
+// b = t / np (mod 256 / np), then a pairwise tree in shared memory adds the
+// 256 / np group sums.  The result does not depend on block timing.
 __device__ __forceinline__ void reduce_partials(const double2 *__restrict__ part, unsigned nblk, int stride,
                                                 int nout, double2 *res)
 {
-    __shared__ double2 acc[8][32];
-    const int g = threadIdx.x >> 5, o = threadIdx.x & 31;
+    __shared__ double2 acc[256];
+    int np = 1;
+    while (np < nout) np <<= 1;
+    const int groups = 256 / np;
+    const int o = threadIdx.x % np, g = threadIdx.x / np;
     double sx = 0.0, sy = 0.0;
     if (o < nout) {
-#pragma unroll 8
-        for (unsigned b = g; b < nblk; b += 8) {
+#pragma unroll 4
+        for (unsigned b = g; b < nblk; b += groups) {
             const double2 v = __ldcg(part + (int64_t)b * stride + o);
             sx += v.x;
             sy += v.y;
         }
     }
-    acc[g][o] = make_double2(sx, sy);
+    acc[threadIdx.x] = make_double2(sx, sy);
     __syncthreads();
-    if ((int)threadIdx.x < nout) {
-        double x = 0.0, y = 0.0;
-        for (int k = 0; k < 8; ++k) {
-            x += acc[k][threadIdx.x].x;
-            y += acc[k][threadIdx.x].y;
+    for (int half = groups >> 1; half > 0; half >>= 1) {
+        if (g < half) {
+            const double2 u = acc[threadIdx.x + half * np];
+            acc[threadIdx.x].x += u.x;
+            acc[threadIdx.x].y += u.y;
         }
-        res[threadIdx.x] = make_double2(x, y);
+        __syncthreads();
     }
+    if ((int)threadIdx.x < nout) res[threadIdx.x] = acc[threadIdx.x];
     __syncthreads();
+}
+
+// Grid of the fused single-launch reductions: up to 8 blocks of 256 per
+// SM, capped so blocks x (outputs rounded to a power of two) fits the
+// kSmallBlocks x 32 partials the scratch holds.
+// One full wave: SMs x resident 256-thread blocks of the kernel (cached per
+// kernel and device).
+template <auto kernel>
+int wave_blocks()
+{
+    static int cache[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 296;
+    if (!cache[dev]) {
+        int sms = 0, per = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, 0);
+        cache[dev] = std::max(1, sms) * std::max(1, std::min(per, 8));
+    }
+    return cache[dev];
+}
+
+template <auto kernel>
+int fused_blocks(int64_t len, int nout)
+{
+    int np = 1;
+    while (np < nout) np <<= 1;
+    const int64_t cap = std::min<int64_t>(wave_blocks<kernel>(), (int64_t)kSmallBlocks * 32 / np);
+    return (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, cap));
 }
 
 // G = op(L)^T R for nl*nr <= NLM*NRM <= 32, register accumulation over a
@@ -514,6 +548,65 @@ __global__ void __launch_bounds__(256)
         for (int o = threadIdx.x; o < nl * nr; o += blockDim.x) {
             const int i = o / nr, j = o % nr;
             out[i + (int64_t)ldo * j] = res[i * NRM + j];
+        }
+        if (threadIdx.x == 0) *ticket = 0u;
+    }
+}
+
+// G = op(L)^T R for up to 16 tiles of NLM x NRM outputs (nl*nr <= 512):
+// block b works on tile g = b % ntiles over the rows of row-block
+// b / ntiles, so the blocks that read the same rows run side by side and
+// share them through L2.  Partials of block b at work + 1 + 32*b; the last
+// block reduces each tile in a fixed order.
+template <class S, int NLM, int NRM>
+__global__ void __launch_bounds__(256)
+    gram_grouped(const __grid_constant__ ColListT<S> L, const __grid_constant__ ColListT<S> R, int64_t len,
+                 int herm, int ngl, int ntiles, double2 *__restrict__ work, double2 *__restrict__ out, int ldo)
+{
+    const int g = blockIdx.x % ntiles, rb = blockIdx.x / ntiles, nrb = gridDim.x / ntiles;
+    const int li0 = (g % ngl) * NLM, rj0 = (g / ngl) * NRM;
+    const int nl = min(NLM, L.n - li0), nr = min(NRM, R.n - rj0);
+    double ar[NLM * NRM], ai[NLM * NRM];
+#pragma unroll
+    for (int k = 0; k < NLM * NRM; ++k) ar[k] = ai[k] = 0.0;
+    const double sg = herm ? -1.0 : 1.0;
+    const int64_t stride = (int64_t)nrb * blockDim.x;
+    for (int64_t r = (int64_t)rb * blockDim.x + threadIdx.x; r < len; r += stride) {
+        double2 rv[NRM];
+#pragma unroll
+        for (int j = 0; j < NRM; ++j) rv[j] = (j < nr) ? col_elem(R, rj0 + j, r) : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int i = 0; i < NLM; ++i) {
+            if (i < nl) {
+                double2 lv = col_elem(L, li0 + i, r);
+                lv.y *= sg;
+#pragma unroll
+                for (int j = 0; j < NRM; ++j) {
+                    const int k = i * NRM + j;
+                    ar[k] = fma(lv.x, rv[j].x, ar[k]);
+                    ar[k] = fma(-lv.y, rv[j].y, ar[k]);
+                    ai[k] = fma(lv.x, rv[j].y, ai[k]);
+                    ai[k] = fma(lv.y, rv[j].x, ai[k]);
+                }
+            }
+        }
+    }
+    unsigned *ticket = reinterpret_cast<unsigned *>(work);
+    double2 *part = work + 1;
+    constexpr int nout = NLM * NRM;
+    block_sum<nout>(ar, ai, part + (int64_t)blockIdx.x * 32, nout);
+    if (last_block(ticket, gridDim.x)) {
+        __shared__ double2 res[32];
+        for (int t = 0; t < ntiles; ++t) {
+            // tile t's partials: blocks t, t + ntiles, ... (stride ntiles*32)
+            reduce_partials(part + (int64_t)t * 32, nrb, ntiles * 32, nout, res);
+            const int ti0 = (t % ngl) * NLM, tj0 = (t / ngl) * NRM;
+            const int tnl = min(NLM, L.n - ti0), tnr = min(NRM, R.n - tj0);
+            for (int o = threadIdx.x; o < tnl * tnr; o += blockDim.x) {
+                const int i = o / tnr, j = o % tnr;
+                out[(ti0 + i) + (int64_t)ldo * (tj0 + j)] = res[i * NRM + j];
+            }
+            __syncthreads();
         }
         if (threadIdx.x == 0) *ticket = 0u;
     }
@@ -646,7 +739,7 @@ __global__ void __launch_bounds__(256)
 // v <- (v - Vp d2)/|w| where |w|^2 = |u|^2 - |d2|^2 (Pythagoras; u is the
 // pass-1 vector, whose component in span(Qp) is already at rounding level,
 // so the subtraction loses nothing).
-template <class S>
+template <class S, int MM>
 __global__ void __launch_bounds__(256)
     gs_pass2(const __grid_constant__ GsArgs<S> A, const double2 *__restrict__ d2, int64_t len, double2 *cout)
 {
@@ -664,14 +757,22 @@ __global__ void __launch_bounds__(256)
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
         double2 q = ldp(A.q + r), v = ldp(A.v + r);
-        for (int i = 0; i < A.m; ++i) {
-            const double2 c = ds[i];
-            const double2 a = ldp(A.qp[i] + r), b = ldp(A.vp[i] + r);
-            q.x -= a.x * c.x - a.y * c.y;
-            q.y -= a.x * c.y + a.y * c.x;
-            v.x -= b.x * c.x - b.y * c.y;
-            v.y -= b.x * c.y + b.y * c.x;
-        }
+        double2 a[MM], b[MM];  // all loads first: MM independent requests in flight
+#pragma unroll
+        for (int i = 0; i < MM; ++i)
+            if (i < A.m) {
+                a[i] = ldp(A.qp[i] + r);
+                b[i] = ldp(A.vp[i] + r);
+            }
+#pragma unroll
+        for (int i = 0; i < MM; ++i)
+            if (i < A.m) {
+                const double2 c = ds[i];
+                q.x -= a[i].x * c.x - a[i].y * c.y;
+                q.y -= a[i].x * c.y + a[i].y * c.x;
+                v.x -= b[i].x * c.x - b[i].y * c.y;
+                v.y -= b[i].x * c.y + b[i].y * c.x;
+            }
         A.q[r] = st2<S>(q.x * sc, q.y * sc);
         A.v[r] = st2<S>(v.x * sc, v.y * sc);
     }
@@ -803,14 +904,16 @@ int stream_blocks(int64_t len)
 
 int64_t gram_work_elems(int nl, int nr, int64_t len)
 {
-    return 1 + std::max<int64_t>((int64_t)gram_blocks(nl, nr, len) * nl * nr, (int64_t)kSmallBlocks * 32);
+    // tiled partials, or one 32-output partial per block of a fused launch
+    // (at most one wave: 8 blocks on each of up to 512 SMs)
+    return 1 + std::max<int64_t>((int64_t)gram_blocks(nl, nr, len) * nl * nr, 4096LL * 32);
 }
 
 template <int A, int B, class S>
 static cudaError_t gram_small_go(const ColListT<S> &L, const ColListT<S> &R, int64_t len, int herm, double2 *out,
                                  int ldo, double2 *work, cudaStream_t st)
 {
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, kSmallBlocks));
+    const int blocks = fused_blocks<gram_small<S, A, B>>(len, A * B);
     gram_small<S, A, B><<<blocks, 256, 0, st>>>(L, R, len, herm, work, out, ldo);
     count_launch();
     return cudaGetLastError();
@@ -829,7 +932,7 @@ static cudaError_t gs_update_go(const S *const *qp, const S *const *vp, int m, S
     A.q = q;
     A.v = v;
     A.m = m;
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, kSmallBlocks));
+    const int blocks = fused_blocks<gs_update<S>>(len, 1);
     gs_update<S><<<blocks, 256, 0, st>>>(A, d, len, work, cout);
     count_launch();
     cudaError_t e = cudaGetLastError();
@@ -852,6 +955,23 @@ cudaError_t gs_update_launch(const float2 *const *qp, const float2 *const *vp, i
 }
 
 template <class S>
+static cudaError_t gram_grouped_go(const ColListT<S> &L, const ColListT<S> &R, int64_t len, int herm, double2 *out,
+                                   int ldo, double2 *work, cudaStream_t st)
+{
+    constexpr int TL = 8, TR = 4;
+    const int ngl = (L.n + TL - 1) / TL, ngr = (R.n + TR - 1) / TR;
+    const int ntiles = ngl * ngr;
+    if (ntiles > 16) return cudaErrorInvalidValue;
+    // one wave of blocks, a whole number of row-blocks per tile
+    const int64_t rows_blocks =
+        std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, wave_blocks<gram_grouped<S, TL, TR>>() / ntiles));
+    gram_grouped<S, TL, TR><<<(unsigned)(rows_blocks * ntiles), 256, 0, st>>>(L, R, len, herm, ngl, ntiles, work, out,
+                                                                             ldo);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <class S>
 static cudaError_t gram_any(const ColListT<S> &L, const ColListT<S> &R, int64_t len, int herm, double2 *out, int ldo,
                             double2 *work, cudaStream_t st)
 {
@@ -868,6 +988,7 @@ static cudaError_t gram_any(const ColListT<S> &L, const ColListT<S> &R, int64_t 
     if (L.n <= 4 && R.n <= 4) return gram_small_go<4, 4>(L, R, len, herm, out, ldo, work, st);
     if (L.n <= 8 && R.n <= 4) return gram_small_go<8, 4>(L, R, len, herm, out, ldo, work, st);
     if (L.n <= 4 && R.n <= 8) return gram_small_go<4, 8>(L, R, len, herm, out, ldo, work, st);
+    if (((L.n + 7) / 8) * ((R.n + 3) / 4) <= 16) return gram_grouped_go(L, R, len, herm, out, ldo, work, st);
     work += 1;  // the tiled path does not use the ticket
     const int nblk = gram_blocks(L.n, R.n, len);
     int64_t chunk = (len + nblk - 1) / nblk;
@@ -993,12 +1114,13 @@ static cudaError_t gs_pass1_go(const S *const *qp, const S *const *vp, int m, S 
     A.q = q;
     A.v = v;
     A.m = m;
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, kSmallBlocks));
-    if (m <= 1) gs_pass1<S, 1><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
-    else if (m <= 2) gs_pass1<S, 2><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
-    else if (m <= 4) gs_pass1<S, 4><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
-    else if (m <= 8) gs_pass1<S, 8><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
-    else gs_pass1<S, 16><<<blocks, 256, 0, st>>>(A, d, len, work, dout);
+#define GS1(MM) gs_pass1<S, MM><<<fused_blocks<gs_pass1<S, MM>>(len, MM + 1), 256, 0, st>>>(A, d, len, work, dout)
+    if (m <= 1) GS1(1);
+    else if (m <= 2) GS1(2);
+    else if (m <= 4) GS1(4);
+    else if (m <= 8) GS1(8);
+    else GS1(16);
+#undef GS1
     count_launch();
     return cudaGetLastError();
 }
@@ -1018,7 +1140,7 @@ template <class S>
 static cudaError_t gs_pass2_go(const S *const *qp, const S *const *vp, int m, S *q, S *v, const double2 *d2,
                                int64_t len, double2 *cout, cudaStream_t st)
 {
-    if (m < 1 || m > 64) return cudaErrorInvalidValue;
+    if (m < 1 || m > 16) return cudaErrorInvalidValue;
     GsArgs<S> A{};
     for (int i = 0; i < m; ++i) {
         A.qp[i] = qp[i];
@@ -1027,7 +1149,12 @@ static cudaError_t gs_pass2_go(const S *const *qp, const S *const *vp, int m, S 
     A.q = q;
     A.v = v;
     A.m = m;
-    gs_pass2<S><<<stream_blocks(len) * 2, 256, 0, st>>>(A, d2, len, cout);
+    const int blocks = stream_blocks(len) * 2;
+    if (m <= 1) gs_pass2<S, 1><<<blocks, 256, 0, st>>>(A, d2, len, cout);
+    else if (m <= 2) gs_pass2<S, 2><<<blocks, 256, 0, st>>>(A, d2, len, cout);
+    else if (m <= 4) gs_pass2<S, 4><<<blocks, 256, 0, st>>>(A, d2, len, cout);
+    else if (m <= 8) gs_pass2<S, 8><<<blocks, 256, 0, st>>>(A, d2, len, cout);
+    else gs_pass2<S, 16><<<blocks, 256, 0, st>>>(A, d2, len, cout);
     count_launch();
     return cudaGetLastError();
 }

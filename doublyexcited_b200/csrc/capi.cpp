@@ -315,6 +315,7 @@ DE_API int de_problem_create(const de_params *pin, de_problem **out)
     hd.vsim = vs.imag();
     hd.sre = scale.real();
     hd.sim = scale.imag();
+    hd.tc = 0;  // the CUDA-core kernels are faster on B200 so far (de_set_matvec_kernel)
 
     auto tinv = cached_tinv(nbig_alloc, nbig_solve, p.nsmall, delta);
     const int nbd = 2 * nbig_alloc + 1;
@@ -392,6 +393,16 @@ DE_API int de_set_stream(de_problem *h, void *s)
 {
     if (!h) return set_error(DE_E_INVALID, "null handle");
     h->stream = s ? (cudaStream_t)s : cudaStreamLegacy;
+    return DE_OK;
+}
+
+DE_API int de_set_matvec_kernel(de_problem *h, int kind)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    if (kind != DE_MATVEC_FMA && kind != DE_MATVEC_TENSOR)
+        return set_error(DE_E_INVALID, "matvec kernel must be DE_MATVEC_FMA or DE_MATVEC_TENSOR (got %d)", kind);
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->ham.tc = kind == DE_MATVEC_TENSOR;
     return DE_OK;
 }
 

@@ -30,6 +30,7 @@ struct HamDev {
     float tf[kMaxNN];
     const float *t1af;
     const float *v12f;
+    int tc;  // 1: axis contractions on the FP64 tensor cores where built (hammult_tc.cu)
 };
 
 // Y(:,:,v) = H X(:,:,v) for v < nvec; vectors are vstride elements apart.
@@ -46,6 +47,14 @@ cudaError_t hammult_pass_launch(const HamDev &h, const double2 *x, double2 *y, i
 // The same on complex64 vectors in FP32 arithmetic (needs h.tf / t1af / v12f).
 cudaError_t hammult_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride, int pass,
                                 cudaStream_t st, double2 shift = double2{0.0, 0.0});
+
+// Tensor-core (DMMA) form of one pass, for the grids hammult_tc_supported
+// accepts; the same arguments and results as hammult_pass_launch.
+bool hammult_tc_supported(int nn);
+cudaError_t hammult_tc_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride, int pass,
+                                   cudaStream_t st, double2 shift);
+cudaError_t hammult_tc_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride, int pass,
+                                   cudaStream_t st, double2 shift);
 
 // One-electron H (NELEC=1): KEMULT1 + V (hammod.F90:71-134).
 cudaError_t hammult1_launch(const HamDev &h, const double *vfull, const double2 *x, double2 *y,

@@ -389,6 +389,25 @@ struct Solver {
         if (e != cudaSuccess) return cuda_error(e, "update");
         return DE_OK;
     }
+    // Y[0..nout) -= sum_i X_i C(i, j) (in place on Y)
+    template <class S>
+    int update_sub(const S *xb, int nin, S *yb, int nout, const double2 *c, int ldc)
+    {
+        UpdListT<S, S> U{};
+        U.nin = nin;
+        U.nout = nout;
+        if (nin > kMaxCols || nout > 16) return set_error(DE_E_INVALID, "update too wide");
+        for (int i = 0; i < nin; ++i) U.x[i] = xb + (int64_t)i * D;
+        for (int j = 0; j < nout; ++j) {
+            U.y[j] = yb + (int64_t)j * D;
+            U.beta[j] = make_double2(1.0, 0.0);
+        }
+        U.alpha = make_double2(-1.0, 0.0);
+        cudaError_t e = update_launch(U, c, ldc, D, st);
+        if (e != cudaSuccess) return cuda_error(e, "update");
+        return DE_OK;
+    }
+
     // H x (the inner solve's callback) and (H - sigma) x
     template <class S>
     int mult_plain(const S *x, S *y, int k)
@@ -416,11 +435,11 @@ struct Solver {
 
     // myhgramschmidt_many with factors (1,0): two classical passes of the
     // (H-sigma)-weighted Gram-Schmidt of the pair (q, v) against the first m
-    // pairs of (LQ, LV).
+    // pairs of (qbase, vbase) (default: the Krylov blocks LQ, LV).
     template <class S>
-    int hgram(int m, S *q, S *v)
+    int hgram(int m, S *q, S *v, S *qbase = nullptr, S *vbase = nullptr)
     {
-        S *LQs = lq_buf<S>(), *LVs = lv_buf<S>();
+        S *LQs = qbase ? qbase : lq_buf<S>(), *LVs = vbase ? vbase : lv_buf<S>();
         std::vector<const S *> qp(m), vp(m);
         for (int i = 0; i < m; ++i) {
             qp[i] = LQs + (int64_t)i * D;
@@ -510,7 +529,24 @@ struct Solver {
             } else {
                 mv_ref += compat ? 1 : k;  // the reference recomputes the product checked above
             }
-            for (int i = 0; i < k; ++i) DE_TRY(hgram(io * k + i, qb + (int64_t)i * D, vb + (int64_t)i * D));
+            const int m0 = io * k;
+            if (k == 1 || m0 == 0) {
+                for (int i = 0; i < k; ++i) DE_TRY(hgram(m0 + i, qb + (int64_t)i * D, vb + (int64_t)i * D));
+            } else {
+                // Block form of the same two-pass classical Gram-Schmidt: the
+                // k new pairs are projected against the m0 earlier pairs as a
+                // block, twice (Q_new -= Q C, V_new -= V C with C = Q^H Q_new),
+                // then orthonormalised among themselves column by column.  In
+                // exact arithmetic this is the reference's column-by-column
+                // result; it reads each earlier vector 6 times per block
+                // instead of 5 times per column.
+                for (int pass = 0; pass < 2; ++pass) {
+                    DE_TRY(gramT(colsT(Q, m0, D), colsT(qb, k, D), dG, m0));
+                    DE_TRY(update_sub(Q, m0, qb, k, dG, m0));
+                    DE_TRY(update_sub(V, m0, vb, k, dG, m0));
+                }
+                for (int i = 0; i < k; ++i) DE_TRY(hgram(i, qb + (int64_t)i * D, vb + (int64_t)i * D, qb, vb));
+            }
         }
         // solution: V (lanham rhs), rhs(:,1,:) = G^{1/2} (:309-316)
         const int thisdim = order * k;

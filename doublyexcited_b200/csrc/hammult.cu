@@ -618,6 +618,7 @@ static cudaError_t pass_go(const HamDev &h, const C2<R> *x, C2<R> *y, int nvec, 
 {
     if (h.nelec != 2 || nvec <= 0) return cudaErrorInvalidValue;
     if (sizeof(R) == 4 && (!h.t1af || !h.v12f)) return cudaErrorInvalidValue;
+    if (h.tc && hammult_tc_supported(h.nn)) return hammult_tc_pass_launch(h, x, y, nvec, vstride, pass, st, shift);
     const CubeArgs<R> a = make_args<R>(h, x, y, vstride, shift);
     const int64_t ncubes = h.m * (int64_t)nvec;
     if (ncubes > 0x7fffffffLL) return cudaErrorInvalidValue;

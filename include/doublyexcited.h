@@ -142,6 +142,12 @@ DE_API int de_set_stream(de_problem *h, void *cuda_stream);
  * contraction + potential; pass B: electron-1 contraction).  Off by default.
  * The reference times phases with MPI_WTIME (gplmr.F90:42-57). */
 DE_API int de_set_profiling(de_problem *h, int on);
+/* Which matvec kernels a handle uses: DE_MATVEC_FMA (the default) the
+ * CUDA-core FMA kernels, DE_MATVEC_TENSOR the axis contractions on the FP64
+ * tensor cores (DMMA) for NN = 9..19 (other grids always use the FMA
+ * kernels).  Both give the reference's H x to rounding. */
+enum { DE_MATVEC_FMA = 0, DE_MATVEC_TENSOR = 1 };
+DE_API int de_set_matvec_kernel(de_problem *h, int kind);
 /* Device milliseconds of pass A and pass B, MATBLOCK calls and vectors
  * multiplied since the last read (waits for the recorded events); resets. */
 DE_API int de_profile_read(de_problem *h, double *pass_a_ms, double *pass_b_ms, int64_t *calls,

@@ -155,3 +155,18 @@ def test_dots(de, oracle):
         c = g.dots(a, b, hermitian=False)
     assert np.max(np.abs(h - a.conj().T @ b)) < 1e-9
     assert np.max(np.abs(c - a.T @ b)) < 1e-9
+
+
+@pytest.mark.parametrize("nb,nk", [(8, 16), (7, 13), (3, 9), (16, 8), (6, 6), (33, 1), (12, 20)])
+def test_dots_shapes(de, nb, nk):
+    """Every Gram path (fused small, grouped tiles, tiled) on ragged shapes,
+    rows not a multiple of any block size."""
+    rng = np.random.default_rng(nb * 100 + nk)
+    n = 300007
+    a = rng.standard_normal((n, nb)) + 1j * rng.standard_normal((n, nb))
+    b = rng.standard_normal((n, nk)) + 1j * rng.standard_normal((n, nk))
+    with de.Problem(n=1, delta=2.0, theta=0.3) as g:
+        h = g.dots(a, b, hermitian=True)
+        c = g.dots(a, b, hermitian=False)
+    assert np.max(np.abs(h - a.conj().T @ b)) < 1e-9
+    assert np.max(np.abs(c - a.T @ b)) < 1e-9

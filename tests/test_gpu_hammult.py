@@ -31,6 +31,24 @@ def test_hammult_matches_oracle_large(de, oracle, n):
     assert rel_err(y, h.matvec(x)) < TOL
 
 
+@pytest.mark.parametrize("kind", ["fma", "tensor"])
+@pytest.mark.parametrize("n", [3, 4, 5, 6, 7])
+def test_both_matvec_kernels_match_oracle(de, oracle, n, kind):
+    """The CUDA-core kernels and the FP64 tensor-core (DMMA) kernels each
+    match the oracle (N=4..9 have both; other grids use the CUDA-core ones)
+    on a block of two vectors with a fused shift."""
+    import torch
+
+    p = oracle.Params(n=n, delta=2.0, theta=0.3)
+    h = oracle.init_hamiltonian(p, nelec=2)
+    x = oracle.seeded_vectors(p.m ** 2, 2, 40 + n)
+    with de.Problem(n=n, delta=2.0, theta=0.3) as g:
+        g.set_matvec_kernel(kind)
+        y = g.matblock(x)
+    for j in range(2):
+        assert rel_err(y[:, j], h.matvec(x[:, j])) < TOL
+
+
 @pytest.mark.parametrize("name", ["hammult_n1.npz", "hammult_n2.npz"])
 def test_hammult_full_golden(de, name):
     meta, a = load_npz(name)
@@ -108,8 +126,9 @@ def test_device_pointer_api(de, oracle):
     assert np.array_equal(y, ref)
 
 
+@pytest.mark.parametrize("kind", ["fma", "tensor"])
 @pytest.mark.parametrize("n,theta", [(3, 0.2), (5, 0.35), (6, 0.2)])
-def test_fp32_matvec_relative_error(de, oracle, n, theta):
+def test_fp32_matvec_relative_error(de, oracle, n, theta, kind):
     """The mixed form's FP32 matvec on complex64 inputs, per call, against
     the FP64 oracle's H x: relative 2-norm error within 1e-6 (FP32 unit
     roundoff 6e-8 times the contraction length and the conditioning of T).
@@ -121,6 +140,7 @@ def test_fp32_matvec_relative_error(de, oracle, n, theta):
     x = oracle.seeded_vectors(p.m ** 2, 2, 21)
     x32 = x.astype(np.complex64)
     with de.Problem(n=n, delta=2.0, theta=theta, precision="mixed") as g:
+        g.set_matvec_kernel(kind)
         g.set_stream(torch.cuda.current_stream().cuda_stream)
         xd = torch.from_numpy(np.ascontiguousarray(x32.T)).cuda()
         yd = torch.empty_like(xd)
@@ -165,3 +185,23 @@ def test_full_size_properties(de, n):
         err = torch.linalg.norm(hxt - hx.view(m, m).t().contiguous().view(-1)) / torch.linalg.norm(hx)
         assert err.item() < 1e-13
         torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("n", [9])
+def test_tensor_and_fma_kernels_agree_at_full_size(de, n):
+    """N=9 (NN=19, 753 MB per vector): the DMMA kernels and the CUDA-core
+    kernels give the same H x to FP64 rounding."""
+    import torch
+
+    with de.Problem(n=n, delta=2.0, theta=0.35) as g:
+        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        gen = torch.Generator(device="cuda").manual_seed(9)
+        x = torch.randn(g.dim, dtype=torch.complex128, device="cuda", generator=gen)
+        y1 = torch.empty_like(x)
+        y2 = torch.empty_like(x)
+        g.set_matvec_kernel("fma")
+        g.matblock_d(x.data_ptr(), y1.data_ptr(), 1)
+        g.set_matvec_kernel("tensor")
+        g.matblock_d(x.data_ptr(), y2.data_ptr(), 1)
+        err = (torch.linalg.norm(y1 - y2) / torch.linalg.norm(y1)).item()
+    assert err < 1e-13
