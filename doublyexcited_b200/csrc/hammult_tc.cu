@@ -110,6 +110,21 @@ __device__ __forceinline__ void load_cube(const TcArgs<R> &a, int64_t cube, TC2<
     }
 }
 
+// Copy cube `cube` into shared buffer xs in its natural order (slab stride
+// NN^2), `nthreads` threads.
+template <int NN, class R, int MODE>
+__device__ __forceinline__ void load_cube_flat(const TcArgs<R> &a, int64_t cube, TC2<R> *xs, int nthreads)
+{
+    constexpr int M = NN * NN * NN;
+    const int64_t vec = cube / M, cc = cube - vec * M;
+    const TC2<R> *xv = a.x + vec * a.vstride;
+    for (int g = threadIdx.x; g < M; g += nthreads) {
+        const TC2<R> *src = (MODE == kTcRowsPot) ? xv + cc + (int64_t)M * g : xv + cc * (int64_t)M + g;
+        if constexpr (sizeof(R) == 8) cp_async_16(xs + g, src);
+        else cp_async_8(xs + g, src);
+    }
+}
+
 // Element offset of (l along axis A, pair pq of the other two coordinates).
 template <int NN, int P2P, int A>
 __device__ __forceinline__ int tc_base(int pq)
@@ -323,6 +338,188 @@ int tc_sm_count()
     return cnt[dev];
 }
 
+// ---------------------------------------------------------------------------
+// Register-tile form (NN = 13, 15).  A warp owns the output tile
+// i in [8a, 8a+8), j in [8b, 8b+8) for every k, with FP64 accumulators in
+// registers for all NN slabs and both components, so the three axis
+// contractions sum in registers and the result leaves the SM once:
+//   axes i and j of slab k:  C_k += T X_k + X_k T      (DMMA: T as A, X_k as
+//                            B; then X_k as A, T as B -- the same C layout)
+//   axis k:                  C_k += sum_l T(k,l) X_l  (FP64 FMA on the
+//                            lane's own two (i, j) positions)
+// The real and imaginary parts are separate real GEMMs (T is real).
+
+template <int NN>
+struct Tc2Cfg {
+    static constexpr int M = NN * NN * NN;
+    static constexpr int P2 = NN * NN;
+    static constexpr int TI = (NN + 7) / 8;  // tiles per axis
+    static constexpr int WARPS = TI * TI;
+    static constexpr int THREADS = 32 * WARPS;
+    static constexpr int KS = (NN + 3) / 4;  // k-steps of 4 over the contracted index
+};
+
+template <int NN, class R, int MODE>
+__global__ void __launch_bounds__(Tc2Cfg<NN>::THREADS, 3)
+    tc2_kernel(const __grid_constant__ HamDev h, const __grid_constant__ TcArgs<R> a, int64_t ncubes)
+{
+    using C = Tc2Cfg<NN>;
+    constexpr int M = C::M, P2 = C::P2, KS = C::KS, TI = C::TI;
+    extern __shared__ __align__(16) unsigned char tc2_smem[];
+    TC2<R> *buf[2] = {reinterpret_cast<TC2<R> *>(tc2_smem), reinterpret_cast<TC2<R> *>(tc2_smem) + M};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ta_ = warp % TI, tb_ = warp / TI;
+    const int q4 = lane & 3, r8 = lane >> 2;
+    // output positions of this lane: i = 8a + lane/4, j = 8b + 2(lane%4) + {0,1}
+    const int oi = 8 * ta_ + r8, oj0 = 8 * tb_ + 2 * q4;
+    // T fragments: TA[ks] = T(i = 8a + lane/4, i' = 4ks + lane%4) (A operand);
+    // TB[ks] = T(j' = 4ks + lane%4, j = 8b + lane/4) (B operand)
+    double TA[KS], TB[KS];
+#pragma unroll
+    for (int ks = 0; ks < KS; ++ks) {
+        const int kk = 4 * ks + q4;
+        const int ri = 8 * ta_ + r8, cj = 8 * tb_ + r8;
+        TA[ks] = (ri < NN && kk < NN) ? h.t[ri > kk ? ri - kk : kk - ri] : 0.0;
+        TB[ks] = (cj < NN && kk < NN) ? h.t[cj > kk ? cj - kk : kk - cj] : 0.0;
+    }
+    // B loads of T X_k: X(i' = 4ks + lane%4, j = 8b + lane/4); A loads of X_k T:
+    // X(i = 8a + lane/4, j' = 4ks + lane%4); own positions (oi, oj0 + {0,1})
+    const int bj = 8 * tb_ + r8, ai_ = 8 * ta_ + r8;
+    const bool own0 = oi < NN && oj0 < NN, own1 = oi < NN && oj0 + 1 < NN;
+    int64_t cube = blockIdx.x;
+    int cur = 0;
+    if (cube < ncubes) load_cube_flat<NN, R, MODE>(a, cube, buf[0], C::THREADS);
+    cp_commit_tc();
+    for (; cube < ncubes; cube += gridDim.x) {
+        const TC2<R> *xs = buf[cur];
+        cp_wait_all_tc();
+        __syncthreads();
+        {  // prefetch the next cube
+            const int64_t nc = cube + gridDim.x;
+            if (nc < ncubes) load_cube_flat<NN, R, MODE>(a, nc, buf[cur ^ 1], C::THREADS);
+            cp_commit_tc();
+        }
+        const R *xr = reinterpret_cast<const R *>(xs);
+        double acc[NN][2][2];  // [k][component][position]
+#pragma unroll
+        for (int k = 0; k < NN; ++k)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) acc[k][c][0] = acc[k][c][1] = 0.0;
+        // axes i and j: k-step by k-step over all slabs, so that the 2*NN
+        // accumulator chains of a step are independent (DMMA latency hidden)
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+            const int kk = 4 * ks + q4;
+            const bool okb = kk < NN && bj < NN, oka = ai_ < NN && kk < NN;
+#pragma unroll
+            for (int l = 0; l < NN; ++l)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const double xb = okb ? (double)xr[2 * (kk + NN * bj + P2 * l) + c] : 0.0;
+                    dmma(acc[l][c][0], acc[l][c][1], TA[ks], xb);
+                }
+#pragma unroll
+            for (int l = 0; l < NN; ++l)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const double xa = oka ? (double)xr[2 * (ai_ + NN * kk + P2 * l) + c] : 0.0;
+                    dmma(acc[l][c][0], acc[l][c][1], xa, TB[ks]);
+                }
+        }
+        // axis k on the lane's own positions
+#pragma unroll
+        for (int l = 0; l < NN; ++l) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const double p0 = own0 ? (double)xr[2 * (oi + NN * oj0 + P2 * l) + c] : 0.0;
+                const double p1 = own1 ? (double)xr[2 * (oi + NN * (oj0 + 1) + P2 * l) + c] : 0.0;
+#pragma unroll
+                for (int k = 0; k < NN; ++k) {
+                    const double t = h.t[k > l ? k - l : l - k];
+                    acc[k][c][0] = fma(t, p0, acc[k][c][0]);
+                    acc[k][c][1] = fma(t, p1, acc[k][c][1]);
+                }
+            }
+        }
+        // epilogue: potential (pass A), 1/SCALE^2, store; lane positions only
+        const int64_t vec = cube / M, cc = cube - vec * M;
+        TC2<R> *yv = a.y + vec * a.vstride;
+        const double s2r = h.s2re, s2i = h.s2im;
+        int ip = 0, jp = 0, kp = 0;
+        double t1p = 0.0;
+        if constexpr (MODE == kTcRowsPot) {
+            ip = (int)(cc % NN);
+            jp = (int)((cc / NN) % NN);
+            kp = (int)(cc / P2);
+            t1p = h.t1a[cc];
+        }
+#pragma unroll
+        for (int pos = 0; pos < 2; ++pos) {
+            const bool own = pos ? own1 : own0;
+            if (!own) continue;
+            const int oj = oj0 + pos;
+#pragma unroll
+            for (int k = 0; k < NN; ++k) {
+                const int g = oi + NN * oj + P2 * k;
+                double ar = acc[k][0][pos], ai = acc[k][1][pos];
+                if constexpr (MODE == kTcRowsPot) {
+                    // V(p,q) (hammod.F90:576-578) times SCALE; the factor
+                    // 1/SCALE^2 below leaves V/SCALE (initmod.F90:224).
+                    constexpr int W = 2 * NN - 1;
+                    const double vr =
+                        (h.t1a[g] + t1p) + h.v12[(oi - ip + NN - 1) + W * ((oj - jp + NN - 1) + W * (k - kp + NN - 1))];
+                    const double pr = vr * h.sre + a.shs.x, pi = vr * h.sim + a.shs.y;
+                    const TC2<R> xe = xs[g];
+                    const double xre = (double)xe.x, xim = (double)xe.y;
+                    ar += pr * xre - pi * xim;
+                    ai += pr * xim + pi * xre;
+                }
+                const double yr = s2r * ar - s2i * ai;
+                const double yi = s2r * ai + s2i * ar;
+                TC2<R> o;
+                if constexpr (MODE == kTcRowsPot) {
+                    o.x = (R)yr;
+                    o.y = (R)yi;
+                    yv[cc + (int64_t)M * g] = o;
+                } else {
+                    TC2<R> &dst = yv[cc * (int64_t)M + g];
+                    const TC2<R> old = dst;
+                    o.x = (R)((double)old.x + yr);
+                    o.y = (R)((double)old.y + yi);
+                    dst = o;
+                }
+            }
+        }
+        cur ^= 1;
+    }
+    cp_wait_all_tc();
+}
+
+template <int NN, class R, int MODE>
+cudaError_t tc2_launch(const HamDev &h, const TcArgs<R> &a, int64_t ncubes, cudaStream_t st)
+{
+    using C = Tc2Cfg<NN>;
+    const size_t smem = 2 * (size_t)C::M * sizeof(TC2<R>);
+    static int per_sm[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!per_sm[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(tc2_kernel<NN, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        int per = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, tc2_kernel<NN, R, MODE>, C::THREADS, smem);
+        if (e != cudaSuccess) return e;
+        per_sm[dev] = std::max(1, per);
+    }
+    const int64_t grid = std::min<int64_t>(ncubes, (int64_t)tc_sm_count() * per_sm[dev]);
+    tc2_kernel<NN, R, MODE><<<(unsigned)grid, C::THREADS, smem, st>>>(h, a, ncubes);
+    count_launch();
+    return cudaGetLastError();
+}
+
+
 template <int NN, class R, int MODE>
 cudaError_t tc_launch(const HamDev &h, const TcArgs<R> &a, int64_t ncubes, cudaStream_t st)
 {
@@ -352,8 +549,8 @@ cudaError_t tc_dispatch(const HamDev &h, const TcArgs<R> &a, int64_t ncubes, cud
     switch (h.nn) {
     case 9: return tc_launch<9, R, MODE>(h, a, ncubes, st);
     case 11: return tc_launch<11, R, MODE>(h, a, ncubes, st);
-    case 13: return tc_launch<13, R, MODE>(h, a, ncubes, st);
-    case 15: return tc_launch<15, R, MODE>(h, a, ncubes, st);
+    case 13: return tc2_launch<13, R, MODE>(h, a, ncubes, st);
+    case 15: return tc2_launch<15, R, MODE>(h, a, ncubes, st);
     case 17: return tc_launch<17, R, MODE>(h, a, ncubes, st);
     case 19: return tc_launch<19, R, MODE>(h, a, ncubes, st);
     default: return cudaErrorInvalidValue;

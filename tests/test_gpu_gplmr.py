@@ -95,6 +95,21 @@ def test_gplmr_mixed_precision_resonance(de, oracle, name):
     assert abs(r.e[0] - complex(*g["e"][0])) < 1e-9
 
 
+@pytest.mark.parametrize("n,theta,spin", [(4, 0.3, "triplet"), (3, 0.45, "triplet"), (4, 0.2, "singlet")])
+def test_mixed_precision_matches_fp64_both_spins(de, oracle, n, theta, spin):
+    """Singlet and triplet starts: the mixed form converges to the FP64
+    form's resonance within 1e-9 Hartree (its inner solve's output is kept
+    in the start block's exchange-symmetry sector)."""
+    p = oracle.Params(n=n, delta=2.0, theta=theta)
+    x0 = oracle.seeded_start(p, 1, 11, spin)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        with de.Problem(n=n, delta=2.0, theta=theta, precision=prec) as h:
+            res[prec] = h.gplmr_eig(x0, -0.7131541429, ns=5, maxit=200, tol=1e-9)
+        assert res[prec].converged, (prec, res[prec].max_residual)
+    assert abs(res["mixed"].e[0] - res["fp64"].e[0]) < 1e-9
+
+
 def test_mixed_precision_first_column_only_mode_is_unsupported(de, oracle):
     g = load_json("gplmr_n3_nev4_compat.json")
     with pytest.raises(de.DeError) as e:
