@@ -1,22 +1,33 @@
 #!/usr/bin/env python
-"""Benchmark: converged helium resonance solves per second on B200.
+"""Benchmark: converged helium resonance solves per second on B200, mixed
+precision against plain FP64.
 
 Workload (default ``solve-n6``): the reference's own logged configuration
 (CSCALE-WORK/Outs/Out.S.D2d0.T0.2d0.N6.petsc: singlet, N=6 so NN=13 points
 per axis and a 4,826,809-dimensional two-electron space, DELTA=2, THETA=0.2,
 GPLMR with NEV=1, NS=5 and the BASIC inner solve of order 5, shift
--0.7131541429), solved to a residual of 1e-8 (|dE| ~ 1e-9 Hartree) from a
-seeded complex-Gaussian singlet start vector.  One step = one solve.
+-0.7131541429), solved to a residual of 1e-8 from a seeded complex-Gaussian
+singlet start vector.  One step = one solve.  The headline is the mixed form
+(``--precision mixed``: complex64 inner solve, FP64 outer iteration); the
+plain FP64 form is timed beside it on the same start vector and the line
+reports both rates and |dE| between them.
 
   value  solves/s with the start vector already in HBM (de_gplmr_eig_d)
   e2e    solves/s through the C ABI with host buffers (de_gplmr_eig: the
          start vector is copied host->device and the Ritz vector back)
-  roofline  the dominant kernel, the FP64 matvec (two passes per vector),
-         timed with CUDA events on its stream over the timed region
+  roofline  the dominant kernel (the FP32 matvec in the mixed form, the FP64
+         matvec in the plain form; two passes per vector), timed with CUDA
+         events recorded by the library on its stream over the timed region;
+         the other matvec is reported beside it
   cpu_baseline  the oracle's HAMMULT (the reference's KEMULT2 loop structure
          in C with OpenMP, all host cores) on a bounded sample of matvecs,
          converted with the solve's HAMMULT count; block operations are not
          charged, so it is a lower bound on the CPU solve time
+
+Other workloads: ``matvec-n9`` / ``matvec-n8`` / ``matvec-n6`` (one step =
+H applied to a block of vectors, FP64 and FP32 with the relative error per
+call, CUDA-core and tensor-core kernels), and ``serve`` (a seeded Poisson
+stream of uneven solve requests through the server: solves/s, p50/p99).
 
 ``--impl reference`` runs that CPU path alone (rank 0) and prints its line.
 Multi-GPU: independent replicas (one solve stream per rank, no collective
@@ -48,6 +59,15 @@ WORKLOADS = {
                           seed=2, spin="singlet", maxit=200, iters_ref=None),
 }
 
+# Block-matvec throughput (one step = H applied to a block of vectors): the
+# FP64 plain matvec and the mixed form's complex64 matvec on the same block,
+# with the mixed result's relative error against the FP64 one per call.
+MATVEC = {
+    "matvec-n9": dict(n=9, theta=0.35, nvec=16, seed=1),
+    "matvec-n8": dict(n=8, theta=0.35, nvec=16, seed=1),
+    "matvec-n6": dict(n=6, theta=0.35, nvec=2, seed=1),  # small case for kernel captures
+}
+
 
 # Served stream: Poisson arrivals of uneven solve requests (seeded); sizes
 # are the batched configuration's mix scaled to grids a few-minute run can
@@ -57,7 +77,7 @@ WORKLOADS = {
 # whose inner-solve Gram matrix fails the reference's 1e-10 self-check).
 SERVE = dict(requests=40, rate=40.0, seed=4, ns=[3, 4, 5, 6], n_weights=[0.2, 0.3, 0.3, 0.2],
              thetas=[0.20, 0.25, 0.30, 0.35, 0.40, 0.45, 0.50], nevs=[1], spins=["singlet", "triplet"],
-             sigma=-0.7131541429, tol=1e-8, maxit=120, workers=4)
+             sigma=-0.7131541429, tol=1e-9, maxit=200, workers=4)
 
 
 def serve_requests(cfg):
@@ -129,8 +149,9 @@ def alg_bytes(nn):
 
 
 # dram bytes (read + write) per vector-matvec (pass A + pass B), keyed by
-# (NN, storage), from the ncu captures summarised under profiles/.
-NCU_TRAFFIC_PER_VECTOR = {}
+# (NN, storage), from the ncu capture of the block-of-2 matvec at N=6
+# (profiles/stream_kernel_matvec-n6.md): both passes' bytes over 2 vectors.
+NCU_TRAFFIC_PER_VECTOR = {(13, "f64"): 343.25e6, (13, "f32"): 151.75e6}
 
 
 class ClockSampler:
@@ -281,6 +302,128 @@ def run_reference(a, w):
     return 0
 
 
+def matvec_main(a):
+    """--workload matvec-*: block MATBLOCK throughput, FP64 and mixed (FP32)
+    on the CUDA-core kernels (the default), the FP64 tensor-core kernels
+    beside; value = FP64 vector-matvecs/s on the device."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import doublyexcited_b200 as de
+    from doublyexcited_b200._lib import check, lib
+
+    rank, world, local = dist_setup()
+    w = MATVEC[a.workload]
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        t = []
+        for _ in range(a.steps):
+            tm, cores = cpu_matvec_seconds(dict(n=w["n"], delta=2.0, theta=w["theta"], seed=w["seed"],
+                                                spin="singlet"), 1)
+            t.append(tm)
+        v = 1.0 / statistics.median(t)
+        print(json.dumps({"impl": "reference", "metric": "vector-matvecs/s", "value": v, "unit": "matvecs/s",
+                          "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 / v,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": {"workload": a.workload, **w},
+                          "cpu_baseline": {"value": v, "unit": "matvecs/s", "cores": cores, "kind": "port",
+                                           "sample": f"{a.steps} oracle HAMMULTs (C, OpenMP, all cores)"},
+                          "e2e": {"value": v, "unit": "matvecs/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return 0
+    torch.cuda.set_device(local)
+    nn = 2 * w["n"] + 1
+    nv = w["nvec"]
+    st = torch.cuda.current_stream()
+    gen = torch.Generator(device="cuda").manual_seed(w["seed"])
+    out = {}
+    clocks = None
+    launches = 0
+    with de.Problem(n=w["n"], delta=2.0, theta=w["theta"], device=local) as g64, \
+            de.Problem(n=w["n"], delta=2.0, theta=w["theta"], device=local, precision="mixed") as g32:
+        dim = g64.dim
+        x = torch.randn(nv, dim, dtype=torch.complex128, device="cuda", generator=gen)
+        y = torch.empty_like(x)
+        x32 = x.to(torch.complex64)
+        y32 = torch.empty_like(x32)
+        for g in (g64, g32):
+            g.set_stream(st.cuda_stream)
+
+        def timed(fn, steps):
+            for _ in range(a.warmup):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(steps):
+                fn()
+            e1.record(st)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / 1e3 / steps
+
+        f64 = lambda: g64.matblock_d(x.data_ptr(), y.data_ptr(), nv)  # noqa: E731
+        f32 = lambda: g32.matblock32_d(x32.data_ptr(), y32.data_ptr(), nv)  # noqa: E731
+        sampler = ClockSampler(local)
+        sampler.start()
+        l0 = lib().de_kernel_launches()
+        t64 = timed(f64, a.steps)
+        launches = (lib().de_kernel_launches() - l0) * a.steps // (a.steps + a.warmup)
+        clocks = sampler.stop()
+        t32 = timed(f32, a.steps)
+        rel = []
+        for j in range(nv):
+            rel.append((torch.linalg.norm(y32[j].to(torch.complex128) - y[j]) / torch.linalg.norm(y[j])).item())
+        g64.set_matvec_kernel("tensor")
+        g32.set_matvec_kernel("tensor")
+        t64tc = timed(f64, a.steps)
+        t32tc = timed(f32, a.steps)
+        g64.set_matvec_kernel("fma")
+        # end to end: host buffers through de_matblock (H2D + D2H per step)
+        xh = x.cpu().numpy().T.copy(order="F")
+        yh = np.empty_like(xh)
+        t0 = time.perf_counter()
+        e2e_steps = max(1, min(a.steps, 2))
+        for _ in range(e2e_steps):
+            check(lib().de_matblock(g64.handle, ctypes.c_void_p(xh.ctypes.data), ctypes.c_void_p(yh.ctypes.data),
+                                    g64.m, dim // g64.m, nv), "de_matblock")
+        torch.cuda.synchronize()
+        t_e2e = (time.perf_counter() - t0) / e2e_steps
+    peak64, peak32 = fp64_peak_tflops(torch), fp32_peak_tflops(torch)
+    fl = alg_flops(nn) * nv
+
+    def roof(t, pk, ebytes, kernel):
+        ach = fl / t / 1e12
+        return {"bound": "tensor" if ebytes == 32 else "fp32-fma", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                "frac": ach / pk, "traffic": NCU_TRAFFIC_PER_VECTOR.get((nn, "f64" if ebytes == 32 else "f32")),
+                "kernel": kernel, "ms_per_vector": t / nv * 1e3,
+                "achieved_gbs_alg": ebytes * nn ** 6 * nv / t / 1e9}
+
+    cpu = None
+    if not a.no_cpu_baseline:
+        tm, cores = cpu_matvec_seconds(dict(n=w["n"], delta=2.0, theta=w["theta"], seed=w["seed"], spin="singlet"), 1)
+        cpu = {"value": 1.0 / tm, "unit": "matvecs/s", "cores": cores, "kind": "port",
+               "sample": f"1 oracle HAMMULT at N={w['n']} (C, OpenMP over columns, {cores} threads)"}
+    line = {"metric": "vector-matvecs/s", "value": nv / t64, "unit": "matvecs/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": t64 * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded complex-Gaussian block)",
+            "config": {"workload": a.workload, **w, "NN": nn, "dim": nn ** 6,
+                       "l2": f"block of {nv} x {16 * nn ** 6 / 1e6:.0f} MB"},
+            "e2e": {"value": nv / t_e2e, "unit": "matvecs/s", "h2d_bytes_per_step": int(xh.nbytes),
+                    "d2h_bytes_per_step": int(yh.nbytes)},
+            "roofline": roof(t64, peak64, 32, "hammult stream_kernel<double> pass A + pass B"),
+            "mixed": {"value": nv / t32, "unit": "matvecs/s", "speedup_vs_fp64": t64 / t32,
+                      "rel_err_vs_fp64_max": max(rel),
+                      "roofline": roof(t32, peak32, 16, "hammult stream_kernel<float> pass A + pass B")},
+            "tensor_cores": {"fp64_value": nv / t64tc, "mixed_value": nv / t32tc,
+                             "fp64_roofline": roof(t64tc, peak64, 32, "hammult tc kernels <double> (DMMA)")},
+            "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
 def serve_main(a):
     """--workload serve: the served stream, mixed and FP64 back to back on one
     GPU, one JSON line.  value = mixed solves/s over the stream."""
@@ -328,7 +471,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="solve-n6", choices=sorted(WORKLOADS) + ["serve"])
+    ap.add_argument("--workload", default="solve-n6", choices=sorted(WORKLOADS) + sorted(MATVEC) + ["serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: FP32 inner solve, FP64 outer iteration (the product form); fp64: plain")
@@ -339,6 +482,8 @@ def main():
     a = ap.parse_args()
     if a.workload == "serve":
         return serve_main(a)
+    if a.workload in MATVEC:
+        return matvec_main(a)
     w = dict(WORKLOADS[a.workload])
     if a.maxit is not None:
         w["maxit"] = a.maxit

@@ -342,6 +342,12 @@ struct SCfg {
     static constexpr int NG = (NN + G - 1) / G;  // groups per cube
     static constexpr int MINB = NT <= 256 ? 2 : 1;
 };
+// complex64 storage needs fewer registers: one more resident CTA per SM
+template <int NN, class R>
+constexpr int smin_blocks()
+{
+    return SCfg<NN>::MINB + ((sizeof(R) == 4 && SCfg<NN>::NT <= 256) ? 1 : 0);
+}
 
 // Asynchronous global -> shared copy of one complex element (16 bytes for
 // complex128, 8 for complex64).
@@ -425,6 +431,21 @@ __device__ __forceinline__ void stream_groups(const HamDev &h, const CubeArgs<R>
             }
             cp_commit();
         }
+        // pass A: this group's potential values, loaded now so that the
+        // table latency hides behind the line work
+        R vpre[GK];
+        if constexpr (MODE == kRowsPot) {
+            if (t < P2) {
+                constexpr int W = 2 * NN - 1;
+                const int oi = t % NN, oj = t / NN;
+#pragma unroll
+                for (int s = 0; s < GK; ++s) {
+                    const int l = L0 + s;
+                    vpre[s] = (t1a_tab<R>(h)[t + P2 * l] + t1p) +
+                              v12_tab<R>(h)[(oi - ip + NN - 1) + W * ((oj - jp + NN - 1) + W * (l - kp + NN - 1))];
+                }
+            }
+        }
         cp_wait<1>();
         __syncthreads();
         const C2<R> *slabs = ring + (size_t)half * G * P2;
@@ -463,11 +484,7 @@ __device__ __forceinline__ void stream_groups(const HamDev &h, const CubeArgs<R>
                 if constexpr (MODE == kRowsPot) {
                     // V(p,q) (hammod.F90:576-578) times SCALE: the final factor
                     // 1/SCALE^2 leaves V/SCALE (initmod.F90:224).
-                    constexpr int W = 2 * NN - 1;
-                    const int oi = t % NN, oj = t / NN;
-                    const int e = t + P2 * l;
-                    const R vr = (t1a_tab<R>(h)[e] + t1p) +
-                                 v12_tab<R>(h)[(oi - ip + NN - 1) + W * ((oj - jp + NN - 1) + W * (l - kp + NN - 1))];
+                    const R vr = vpre[s];
                     const R pr = vr * (R)h.sre + (R)a.shs.x, pi = vr * (R)h.sim + (R)a.shs.y;
                     ar[l] += pr * v.x - pi * v.y;
                     ai[l] += pr * v.y + pi * v.x;
@@ -489,7 +506,7 @@ __device__ __forceinline__ void stream_groups(const HamDev &h, const CubeArgs<R>
 }
 
 template <class R, int NN, int MODE>
-__global__ void __launch_bounds__(SCfg<NN>::NT, SCfg<NN>::MINB)
+__global__ void __launch_bounds__(SCfg<NN>::NT, (smin_blocks<NN, R>()))
     stream_kernel(const __grid_constant__ HamDev h, const __grid_constant__ CubeArgs<R> a, int64_t ncubes)
 {
     using C = SCfg<NN>;
@@ -566,7 +583,7 @@ cudaError_t launch_stream(const HamDev &h, const CubeArgs<R> &a, int64_t ncubes,
         if (e != cudaSuccess) return e;
         attr[dev] = true;
     }
-    const int64_t grid = std::min<int64_t>(ncubes, (int64_t)sm_count() * C::MINB);
+    const int64_t grid = std::min<int64_t>(ncubes, (int64_t)sm_count() * smin_blocks<NN, R>());
     stream_kernel<R, NN, MODE><<<(unsigned)grid, C::NT, smem, st>>>(h, a, ncubes);
     count_launch();
     return cudaGetLastError();
