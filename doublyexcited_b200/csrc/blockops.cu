@@ -35,9 +35,8 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b)
 
 // ---------------------------------------------------------------- Gram
 
-constexpr int kGramRT = 32;  // rows per smem tile
+constexpr int kGramRT = 32;  // row granularity of the Gram split over blocks
 constexpr int kSmallBlocks = 296;  // grid of the fused small reductions
-constexpr int kGramTX = 16;  // thread grid 16 x 16
 
 // element load widened to FP64
 __device__ __forceinline__ double2 ld2(const double2 *p) { return __ldg(p); }
@@ -78,75 +77,6 @@ __device__ __forceinline__ double2 col_elem(const ColListT<S> &L, int c, int64_t
     return v;
 }
 
-template <class S, int TA, int TB>
-__global__ void __launch_bounds__(256)
-    gram_partial(const __grid_constant__ ColListT<S> L, const __grid_constant__ ColListT<S> R, int64_t len,
-                 int64_t chunk, int herm, double2 *__restrict__ work)
-{
-    extern __shared__ double2 gsm[];
-    const int nl = L.n, nr = R.n;
-    double2 *ls = gsm;                  // [RT][nl]
-    double2 *rs = gsm + kGramRT * nl;   // [RT][nr]
-    const int tx = threadIdx.x % kGramTX, ty = threadIdx.x / kGramTX;
-    double ar[TA][TB], ai[TA][TB];
-#pragma unroll
-    for (int a = 0; a < TA; ++a)
-#pragma unroll
-        for (int b = 0; b < TB; ++b) ar[a][b] = ai[a][b] = 0.0;
-    const int64_t r0 = (int64_t)blockIdx.x * chunk;
-    const int64_t r1 = min(len, r0 + chunk);
-    const double sg = herm ? -1.0 : 1.0;  // conj(L) flips the sign of L.im
-    for (int64_t rt = r0; rt < r1; rt += kGramRT) {
-        const int rows = (int)min((int64_t)kGramRT, r1 - rt);
-        for (int idx = threadIdx.x; idx < kGramRT * nl; idx += blockDim.x) {
-            const int r = idx % kGramRT, c = idx / kGramRT;
-            double2 v = make_double2(0.0, 0.0);
-            if (r < rows) v = col_elem(L, c, rt + r);
-            v.y *= sg;
-            ls[r * nl + c] = v;
-        }
-        for (int idx = threadIdx.x; idx < kGramRT * nr; idx += blockDim.x) {
-            const int r = idx % kGramRT, c = idx / kGramRT;
-            double2 v = make_double2(0.0, 0.0);
-            if (r < rows) v = col_elem(R, c, rt + r);
-            rs[r * nr + c] = v;
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int r = 0; r < kGramRT; ++r) {
-            double2 lv[TA], rv[TB];
-#pragma unroll
-            for (int a = 0; a < TA; ++a) {
-                const int i = tx + kGramTX * a;
-                lv[a] = (i < nl) ? ls[r * nl + i] : make_double2(0.0, 0.0);
-            }
-#pragma unroll
-            for (int b = 0; b < TB; ++b) {
-                const int j = ty + kGramTX * b;
-                rv[b] = (j < nr) ? rs[r * nr + j] : make_double2(0.0, 0.0);
-            }
-#pragma unroll
-            for (int a = 0; a < TA; ++a)
-#pragma unroll
-                for (int b = 0; b < TB; ++b) {
-                    ar[a][b] = fma(lv[a].x, rv[b].x, ar[a][b]);
-                    ar[a][b] = fma(-lv[a].y, rv[b].y, ar[a][b]);
-                    ai[a][b] = fma(lv[a].x, rv[b].y, ai[a][b]);
-                    ai[a][b] = fma(lv[a].y, rv[b].x, ai[a][b]);
-                }
-        }
-        __syncthreads();
-    }
-    double2 *out = work + (int64_t)blockIdx.x * nl * nr;
-#pragma unroll
-    for (int a = 0; a < TA; ++a)
-#pragma unroll
-        for (int b = 0; b < TB; ++b) {
-            const int i = tx + kGramTX * a, j = ty + kGramTX * b;
-            if (i < nl && j < nr) out[i + nl * j] = make_double2(ar[a][b], ai[a][b]);
-        }
-}
-
 // One 256-thread block per 32 outputs; warp g sums blocks b = g (mod 8).
 __global__ void __launch_bounds__(256)
     gram_reduce(const double2 *__restrict__ work, int nblk, int nl, int nr, double2 *__restrict__ out, int ldo)
@@ -180,33 +110,6 @@ int gram_blocks(int nl, int nr, int64_t len)
     const int64_t tiles = (len + kGramRT - 1) / kGramRT;
     const int64_t cap = (int64_t)nl * nr > 1024 ? 296 : 148 * 8;
     return (int)std::max<int64_t>(1, std::min(tiles, cap));
-}
-
-template <int TA, int TB, class S>
-cudaError_t gram_go(const ColListT<S> &L, const ColListT<S> &R, int64_t len, int herm, double2 *work,
-                    int nblk, int64_t chunk, cudaStream_t st)
-{
-    const size_t smem = (size_t)kGramRT * (L.n + R.n) * sizeof(double2);
-    static bool attr[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (!attr[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(gram_partial<S, TA, TB>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(kGramRT * (64 + 128) * sizeof(double2)));
-        if (e != cudaSuccess) return e;
-        attr[dev] = true;
-    }
-    gram_partial<S, TA, TB><<<nblk, 256, smem, st>>>(L, R, len, chunk, herm, work);
-    count_launch();
-    return cudaGetLastError();
-}
-
-int round_t(int n)
-{
-    const int t = (n + kGramTX - 1) / kGramTX;
-    return t <= 1 ? 1 : t <= 2 ? 2 : t <= 4 ? 4 : 8;
 }
 
 // ---------------------------------------------------------------- update
@@ -1035,6 +938,137 @@ static cudaError_t gram_grouped_go(const ColListT<S> &L, const ColListT<S> &R, i
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- Gram on the FP64 tensor cores
+// G = op(L)^T R as real GEMMs over the rows on DMMA (mma.sync m8n8k4 f64):
+// with L = Lr + i Li, R = Rr + i Ri,
+//   Re G = Lr^T Rr + s Li^T Ri,  Im G = Lr^T Ri - s Li^T Rr  (s = +1 for
+//   conj(L), -1 for L),
+// A fragments straight from L (lane: row r0 + lane%4, column i0 + lane/4),
+// B fragments from R (row r0 + lane%4, column j0 + lane/4): one 16-byte
+// load gives a lane both components.  A warp owns MTW x NTW 8x8 output
+// tiles; a block holds WM x WN warps covering all outputs, times RG row
+// groups that take interleaved 4-row steps of the block's row range.  Block
+// partials go to work[block][nl*nr] (column-major) for gram_reduce.
+
+__device__ __forceinline__ void dmma_g(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <class S, int MTW, int NTW>
+__global__ void __launch_bounds__(512)
+    gram_tc(const __grid_constant__ ColListT<S> L, const __grid_constant__ ColListT<S> R, int64_t len, int64_t chunk,
+            int herm, int wm, int wn, int rg, double2 *__restrict__ work)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int per = wm * wn;
+    const int g = warp / per, wt = warp - g * per;
+    const int wi = wt % wm, wj = wt / wm;
+    const int nl = L.n, nr = R.n;
+    const double sg = herm ? 1.0 : -1.0;
+    const int q4 = lane & 3, r8 = lane >> 2;
+    double re[MTW][NTW][2], im[MTW][NTW][2];
+#pragma unroll
+    for (int a = 0; a < MTW; ++a)
+#pragma unroll
+        for (int b = 0; b < NTW; ++b) re[a][b][0] = re[a][b][1] = im[a][b][0] = im[a][b][1] = 0.0;
+    const int64_t r0 = (int64_t)blockIdx.x * chunk;
+    const int64_t r1 = min(len, r0 + chunk);
+    for (int64_t rb = r0 + 4 * (int64_t)g; rb < r1; rb += 4 * (int64_t)rg) {
+        const int64_t r = rb + q4;
+        const bool rok = r < r1;
+        double2 lv[MTW], rv[NTW];
+#pragma unroll
+        for (int a = 0; a < MTW; ++a) {
+            const int i = 8 * (wi * MTW + a) + r8;
+            lv[a] = (rok && i < nl) ? col_elem(L, i, r) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int b = 0; b < NTW; ++b) {
+            const int j = 8 * (wj * NTW + b) + r8;
+            rv[b] = (rok && j < nr) ? col_elem(R, j, r) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int a = 0; a < MTW; ++a)
+#pragma unroll
+            for (int b = 0; b < NTW; ++b) {
+                dmma_g(re[a][b][0], re[a][b][1], lv[a].x, rv[b].x);
+                dmma_g(re[a][b][0], re[a][b][1], lv[a].y, sg * rv[b].y);
+                dmma_g(im[a][b][0], im[a][b][1], lv[a].x, rv[b].y);
+                dmma_g(im[a][b][0], im[a][b][1], lv[a].y, -sg * rv[b].x);
+            }
+    }
+    // sum the row groups in shared memory (fixed order), then one partial per block
+    extern __shared__ double2 gtc_sm[];  // [rg][per*32][MTW*NTW*2]
+    constexpr int V = MTW * NTW * 2;
+    double2 *mine = gtc_sm + ((int64_t)g * per * 32 + wt * 32 + lane) * V;
+#pragma unroll
+    for (int a = 0; a < MTW; ++a)
+#pragma unroll
+        for (int b = 0; b < NTW; ++b)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) mine[(a * NTW + b) * 2 + c] = make_double2(re[a][b][c], im[a][b][c]);
+    __syncthreads();
+    if (g == 0) {
+        double2 *part = work + (int64_t)blockIdx.x * nl * nr;
+#pragma unroll
+        for (int a = 0; a < MTW; ++a)
+#pragma unroll
+            for (int b = 0; b < NTW; ++b)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int k = (a * NTW + b) * 2 + c;
+                    double x = 0.0, y = 0.0;
+                    for (int gg = 0; gg < rg; ++gg) {
+                        const double2 v = gtc_sm[((int64_t)gg * per * 32 + wt * 32 + lane) * V + k];
+                        x += v.x;
+                        y += v.y;
+                    }
+                    const int i = 8 * (wi * MTW + a) + r8, j = 8 * (wj * NTW + b) + 2 * q4 + c;
+                    if (i < nl && j < nr) part[i + (int64_t)nl * j] = make_double2(x, y);
+                }
+    }
+}
+
+template <class S, int MTW, int NTW>
+static cudaError_t gram_tc_go(const ColListT<S> &L, const ColListT<S> &R, int64_t len, int herm, double2 *out, int ldo,
+                              double2 *work, cudaStream_t st)
+{
+    const int mt = (L.n + 7) / 8, nt = (R.n + 7) / 8;
+    const int wm = (mt + MTW - 1) / MTW, wn = (nt + NTW - 1) / NTW;
+    const int per = wm * wn;
+    if (per > 16) return cudaErrorInvalidValue;
+    const int rg = std::max(1, 8 / per);
+    const int threads = 32 * per * rg;
+    const size_t smem = (size_t)threads * MTW * NTW * 2 * sizeof(double2);
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(gram_tc<S, MTW, NTW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             512 * MTW * NTW * 2 * (int)sizeof(double2));
+        if (e != cudaSuccess) return e;
+        attr[dev] = true;
+    }
+    // about four blocks per SM; the partials (nblk x nl x nr) fit the work
+    // buffer that gram_work_elems sizes for the tiled path
+    const int nblk = gram_blocks(L.n, R.n, len);
+    int64_t chunk = (len + nblk - 1) / nblk;
+    chunk = (chunk + 3) / 4 * 4;
+    work += 1;
+    gram_tc<S, MTW, NTW><<<nblk, threads, smem, st>>>(L, R, len, chunk, herm, wm, wn, rg, work);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int nout = L.n * R.n;
+    gram_reduce<<<(nout + 31) / 32, 256, 0, st>>>(work, nblk, L.n, R.n, out, ldo);
+    count_launch();
+    return cudaGetLastError();
+}
+
 template <class S>
 static cudaError_t gram_any(const ColListT<S> &L, const ColListT<S> &R, int64_t len, int herm, double2 *out, int ldo,
                             double2 *work, cudaStream_t st)
@@ -1055,25 +1089,12 @@ static cudaError_t gram_any(const ColListT<S> &L, const ColListT<S> &R, int64_t 
     // a few grouped tiles beat the tiled kernel; at 8 x 16 (the K/M projection
     // of NEV = 1) the tiled kernel is faster (2.2 vs 1.2 ms at N = 6)
     if (((L.n + 3) / 4) * ((R.n + 1) / 2) <= 6) return gram_grouped_go(L, R, len, herm, out, ldo, work, st);
-    work += 1;  // the tiled path does not use the ticket
-    const int nblk = gram_blocks(L.n, R.n, len);
-    int64_t chunk = (len + nblk - 1) / nblk;
-    chunk = (chunk + kGramRT - 1) / kGramRT * kGramRT;
-    const int ta = round_t(L.n), tb = round_t(R.n);
-    cudaError_t e;
-    if (ta > 4) return cudaErrorInvalidValue;
-#define GRAM_CASE(A, B) \
-    if (ta == A && tb == B) e = gram_go<A, B>(L, R, len, herm, work, nblk, chunk, st); else
-    GRAM_CASE(1, 1) GRAM_CASE(1, 2) GRAM_CASE(1, 4) GRAM_CASE(1, 8)
-    GRAM_CASE(2, 1) GRAM_CASE(2, 2) GRAM_CASE(2, 4) GRAM_CASE(2, 8)
-    GRAM_CASE(4, 1) GRAM_CASE(4, 2) GRAM_CASE(4, 4) GRAM_CASE(4, 8)
-    return cudaErrorInvalidValue;
-#undef GRAM_CASE
-    if (e != cudaSuccess) return e;
-    const int nout = L.n * R.n;
-    gram_reduce<<<(nout + 31) / 32, 256, 0, st>>>(work, nblk, L.n, R.n, out, ldo);
-    count_launch();
-    return cudaGetLastError();
+    {  // everything else on the FP64 tensor cores
+        const int mt = (L.n + 7) / 8, nt = (R.n + 7) / 8;
+        if (mt == 1 && nt <= 2) return gram_tc_go<S, 1, 2>(L, R, len, herm, out, ldo, work, st);
+        if (mt <= 2 && nt <= 4) return gram_tc_go<S, 1, 2>(L, R, len, herm, out, ldo, work, st);
+        return gram_tc_go<S, 2, 4>(L, R, len, herm, out, ldo, work, st);
+    }
 }
 
 cudaError_t gram_launch(const ColList &L, const ColList &R, int64_t len, int herm, double2 *out, int ldo,
