@@ -57,6 +57,8 @@ WORKLOADS = {
                      seed=0, spin="singlet", maxit=200, iters_ref=52),
     "solve-n8-nev8": dict(n=8, delta=2.0, theta=0.35, nev=8, ns=5, order=5, sigma=-0.78, tol=1e-7,
                           seed=2, spin="singlet", maxit=200, iters_ref=None),
+    "solve-n8-nev8-s060": dict(n=8, delta=2.0, theta=0.35, nev=8, ns=5, order=5, sigma=-0.60, tol=1e-7,
+                               seed=2, spin="singlet", maxit=200, iters_ref=None),
 }
 
 # Block-matvec throughput (one step = H applied to a block of vectors): the
@@ -579,7 +581,12 @@ def main():
         return out
 
     head = measure(a.precision, True)
-    other = measure("fp64", False) if a.precision != "fp64" and not a.no_fp64_compare else None
+    other, other_err = None, None
+    if a.precision != "fp64" and not a.no_fp64_compare:
+        try:
+            other = measure("fp64", False)
+        except de.DeError as exc:  # e.g. the reference's 1e-10 self-check STOP at NEV > 1
+            other_err = str(exc)
     prob, x0, dim = head["prob"], head["x0"], head["dim"]
     elapsed, st, e_final, prof, launches, clocks = (head["elapsed"], head["st"], head["e"], head["prof"],
                                                      head["launches"], head["clocks"])
@@ -646,7 +653,7 @@ def main():
                "sample": f"3 oracle HAMMULTs at N={w['n']} (C, OpenMP over columns, {cores} threads) "
                          f"= {t_mv:.3f} s each, x {nmv} HAMMULTs per solve; block ops not charged"}
 
-    compare = None
+    compare = {"fp64_error": other_err} if other_err else None
     if other is not None:
         de_max = float(np.max(np.abs(np.sort_complex(head["e_all"]) - np.sort_complex(other["e_all"]))))
         compare = {"fp64_value": other["value"], "fp64_ms_per_step": other["elapsed"] / a.steps * 1e3,

@@ -342,7 +342,8 @@ struct SCfg {
     static constexpr int NG = (NN + G - 1) / G;  // groups per cube
     static constexpr int MINB = NT <= 256 ? 2 : 1;
 };
-// complex64 storage needs fewer registers: one more resident CTA per SM
+// complex64 storage needs fewer registers: one more resident CTA per SM (a
+// fourth one at NN=13 fits without spills but measured no faster)
 template <int NN, class R>
 constexpr int smin_blocks()
 {
