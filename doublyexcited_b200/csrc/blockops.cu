@@ -135,7 +135,24 @@ __global__ void __launch_bounds__(256)
             yb[j] = make_double2(0.0, 0.0);
             if (j < nout && (U.beta[j].x != 0.0 || U.beta[j].y != 0.0)) yb[j] = cmul(U.beta[j], ldp(U.y[j] + r));
         }
-        for (int i = 0; i < nin; ++i) {
+        // four input columns a step, their loads issued together
+        int i = 0;
+        for (; i + 4 <= nin; i += 4) {
+            double2 xv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) xv[u] = ldp(U.x[i + u] + r);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int j = 0; j < NOUT; ++j) {
+                    const double2 c = cs[(i + u) * NOUT + j];
+                    acc[j].x = fma(xv[u].x, c.x, acc[j].x);
+                    acc[j].x = fma(-xv[u].y, c.y, acc[j].x);
+                    acc[j].y = fma(xv[u].x, c.y, acc[j].y);
+                    acc[j].y = fma(xv[u].y, c.x, acc[j].y);
+                }
+        }
+        for (; i < nin; ++i) {
             const double2 xv = ldp(U.x[i] + r);
 #pragma unroll
             for (int j = 0; j < NOUT; ++j) {
@@ -183,6 +200,18 @@ __global__ void axpc_kernel(const __grid_constant__ PtrPack P, double2 s, const 
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
         const double2 av = P.a[j][r], bv = P.b[j][r];
         P.out[j][r] = make_double2(av.x + sc.x * bv.x - sc.y * bv.y, av.y + sc.x * bv.y + sc.y * bv.x);
+    }
+}
+
+// out = a + s b over n contiguous elements (FP64 arithmetic, storage S)
+template <class S>
+__global__ void axpy_kernel(S *__restrict__ out, const S *__restrict__ a, const S *__restrict__ b, double2 s,
+                            int64_t n)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+        const double2 av = ldp(a + r), bv = ldp(b + r);
+        out[r] = st2<S>(av.x + s.x * bv.x - s.y * bv.y, av.y + s.x * bv.y + s.y * bv.x);
     }
 }
 
@@ -1090,9 +1119,15 @@ static cudaError_t gram_any(const ColListT<S> &L, const ColListT<S> &R, int64_t 
     // of NEV = 1) the tiled kernel is faster (2.2 vs 1.2 ms at N = 6)
     if (((L.n + 3) / 4) * ((R.n + 1) / 2) <= 6) return gram_grouped_go(L, R, len, herm, out, ldo, work, st);
     {  // everything else on the FP64 tensor cores
+        // warp tiles sized to the output: no more padded tiles than needed
         const int mt = (L.n + 7) / 8, nt = (R.n + 7) / 8;
-        if (mt == 1 && nt <= 2) return gram_tc_go<S, 1, 2>(L, R, len, herm, out, ldo, work, st);
-        if (mt <= 2 && nt <= 4) return gram_tc_go<S, 1, 2>(L, R, len, herm, out, ldo, work, st);
+        if (mt == 1) {
+            if (nt == 1) return gram_tc_go<S, 1, 1>(L, R, len, herm, out, ldo, work, st);
+            if (nt <= 4) return gram_tc_go<S, 1, 2>(L, R, len, herm, out, ldo, work, st);
+            return gram_tc_go<S, 1, 4>(L, R, len, herm, out, ldo, work, st);
+        }
+        if (nt == 1) return gram_tc_go<S, 2, 1>(L, R, len, herm, out, ldo, work, st);
+        if (nt <= 4) return gram_tc_go<S, 2, 2>(L, R, len, herm, out, ldo, work, st);
         return gram_tc_go<S, 2, 4>(L, R, len, herm, out, ldo, work, st);
     }
 }
@@ -1147,6 +1182,22 @@ cudaError_t axpc_launch(double2 *const *out, const double2 *const *a, const doub
         P.b[j] = b[j];
     }
     axpc_kernel<<<dim3(stream_blocks(len) / n + 1, n), 256, 0, st>>>(P, s, c_dev, len);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t axpy_launch(double2 *out, const double2 *a, const double2 *b, double2 s, int64_t n, cudaStream_t st)
+{
+    if (n < 1) return cudaErrorInvalidValue;
+    axpy_kernel<double2><<<stream_blocks(n) * 2, 256, 0, st>>>(out, a, b, s, n);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t axpy_launch(float2 *out, const float2 *a, const float2 *b, double2 s, int64_t n, cudaStream_t st)
+{
+    if (n < 1) return cudaErrorInvalidValue;
+    axpy_kernel<float2><<<stream_blocks(n) * 2, 256, 0, st>>>(out, a, b, s, n);
     count_launch();
     return cudaGetLastError();
 }

@@ -154,6 +154,11 @@ cudaError_t small_hsqrt1_launch(const double2 *g, double2 *ginvh, double2 *gsq, 
 cudaError_t small_ortho_check_launch(const double2 *t, int k, int *flag, cudaStream_t st, double tol = 1e-10);
 cudaError_t small_gemm_launch(const double2 *a, const double2 *b, double2 *c, int m, int k, int n, cudaStream_t st);
 
+// out = a + s b over n contiguous complex elements (may alias a or b
+// element for element).
+cudaError_t axpy_launch(double2 *out, const double2 *a, const double2 *b, double2 s, int64_t n, cudaStream_t st);
+cudaError_t axpy_launch(float2 *out, const float2 *a, const float2 *b, double2 s, int64_t n, cudaStream_t st);
+
 // x_j *= c_j (c from DEVICE, complex), in place.
 cudaError_t scale_cols_launch(double2 *const *x, int n, const double2 *c_dev, int64_t len,
                               cudaStream_t st);

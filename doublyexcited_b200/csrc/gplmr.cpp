@@ -32,8 +32,9 @@
 // converged eigenvalues meet the FP64 tolerance.  The inner solve's
 // orthonormality self-check is held to 1e-3 instead of 1e-10 there.
 #include <algorithm>
-#include <type_traits>
 #include <chrono>
+#include <initializer_list>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -258,6 +259,33 @@ struct Solver {
         return DE_OK;
     }
 
+    // B <- B - Q (Q^H B) with Q the union of mutually orthonormal blocks, in
+    // one classical pass (one Gram, one update; AB likewise with AQ).  The
+    // reference projects block by block (gplmr.F90:127-130,160-165,180-190);
+    // with orthonormal blocks the two agree up to rounding, and this reads
+    // the vectors once instead of once per block.
+    struct QBlk {
+        double2 *v;
+        int k;
+        double2 *av;
+    };
+    int orth_against_all(std::initializer_list<QBlk> qs, double2 *b, int kb, double2 *ab = nullptr)
+    {
+        ColList L{};
+        std::vector<const double2 *> xs, axs;
+        for (const QBlk &q : qs)
+            for (int j = 0; j < q.k; ++j) {
+                L.a[L.n++] = col(q.v, j);
+                xs.push_back(col(q.v, j));
+                if (q.av) axs.push_back(col(q.av, j));
+            }
+        if (L.n == 0) return DE_OK;
+        DE_TRY(gram_dev(L, cols(b, kb, D), dG, L.n));
+        DE_TRY(update(xs, clw(b, kb), dG, L.n, -1.0, 1.0));
+        if (ab) DE_TRY(update(axs, clw(ab, kb), dG, L.n, -1.0, 1.0));
+        return DE_OK;
+    }
+
     // cholQR lamod.f90:128-180 on the device: R = chol(X^H X) (upper), X <- X
     // R^{-1}; R^{-1} stays in dRinv for the following trsm.  Breakdown sets
     // a device flag that the next residual check reports.
@@ -475,6 +503,25 @@ struct Solver {
         return DE_OK;
     }
 
+    // Orthonormalise the k pairs (q_i, v_i) of one Krylov block among
+    // themselves in the q inner product: CholQR twice (G = Q^H Q = R^H R,
+    // Q <- Q R^-1, V <- V R^-1).  The QR factor with a positive real diagonal
+    // is unique, so this is the reference's column-by-column two-pass
+    // Gram-Schmidt (myhgramschmidt_many) to rounding, in 3 passes over the
+    // block instead of k.
+    template <class S>
+    int block_cholqr2(S *qb, S *vb, int k)
+    {
+        for (int pass = 0; pass < 2; ++pass) {
+            DE_TRY(gramT(colsT(qb, k, D), colsT(qb, k, D), dG, k));
+            cudaError_t e = small_cholinv_launch(dG, k, dRinv, dFlags, st);
+            if (e != cudaSuccess) return cuda_error(e, "small_cholinv");
+            DE_TRY(updateT(qb, k, qb, k, dRinv, k));
+            DE_TRY(updateT(vb, k, vb, k, dRinv, k));
+        }
+        return DE_OK;
+    }
+
     int shift_sub(double2 *q, const double2 *v, int k)  // q <- q - sigma v
     {
         const cplx ms = -sigma;
@@ -507,6 +554,7 @@ struct Solver {
             cudaError_t e = small_hsqrt1_launch(dG, dGinvh, dGsq, dFlags, st);
             if (e != cudaSuccess) return cuda_error(e, "small_hsqrt1");
             DE_TRY(updateT(V, 1, V, 1, dGinvh, 1));
+            if (!compat) DE_TRY(updateT(Q, 1, Q, 1, dGinvh, 1));
         } else {
             std::vector<cplx> g, ginv;
             DE_TRY(gram_hostT(colsT(Q, k, D), colsT(Q, k, D), g));
@@ -518,9 +566,18 @@ struct Solver {
                 for (int i = 0; i < k; ++i) ginvh[i + (size_t)k * j] = std::conj(ginv[j + (size_t)k * i]);
             DE_TRY(upload(ginvh, dC));
             DE_TRY(updateT(V, k, V, k, dC, k));
+            if (!compat) DE_TRY(updateT(Q, k, Q, k, dC, k));
         }
-        // self-check: (H - sigma) V_1 orthonormal
-        DE_TRY(mult_shifted(V, Q, k));
+        // self-check: (H - sigma) V_1 orthonormal.  The reference multiplies
+        // again (harmonic_ritz_small.F90:221-242); (H - sigma) is linear, so
+        // the product is Q G^{-1/2}, formed above with the same coefficients
+        // as V (counted as the reference's product; the compatibility mode's
+        // first-column-only product is not linear and is recomputed).
+        if (compat) {
+            DE_TRY(mult_shifted(V, Q, k));
+        } else {
+            mv_ref += k;
+        }
         DE_TRY(gramT(colsT(Q, k, D), colsT(Q, k, D), dT, k));
         {
             cudaError_t e = small_ortho_check_launch(dT, k, dFlags, st, ortho_tol);
@@ -529,14 +586,27 @@ struct Solver {
         // fast_harmritz_setup :86-158 (maxiter = M^2 never truncates a block)
         for (int io = 0; io < order; ++io) {
             S *vb = V + (int64_t)io * k * D, *qb = Q + (int64_t)io * k * D;
-            if (io > 0) {
+            if (io > 0 && !compat) {
+                // H v_{io-1} = (H - sigma) v_{io-1} + sigma v_{io-1} = q_{io-1} + sigma v_{io-1}:
+                // the Gram-Schmidt steps apply the same combinations to q and
+                // v, so q_i = (H - sigma) v_i holds for every finished column
+                // and the reference's product H v_{io-1} (harmonic_ritz_small.F90:
+                // 119-126) is an axpy; stats.matvecs_reference keeps counting it.
+                mv_ref += k;
+                cudaError_t e = axpy_launch(vb, Q + (int64_t)(io - 1) * k * D, V + (int64_t)(io - 1) * k * D,
+                                            make_double2(sigma.real(), sigma.imag()), (int64_t)k * D, st);
+                if (e != cudaSuccess) return cuda_error(e, "axpy");
+                DE_TRY(mult_shifted(vb, qb, k));
+            } else if (io > 0) {
                 DE_TRY(mult_plain(V + (int64_t)(io - 1) * k * D, vb, k));
                 DE_TRY(mult_shifted(vb, qb, k));
             } else {
                 mv_ref += compat ? 1 : k;  // the reference recomputes the product checked above
             }
             const int m0 = io * k;
-            if (k == 1 || m0 == 0) {
+            if (k > 1 && m0 == 0 && !compat) {
+                DE_TRY(block_cholqr2(qb, vb, k));
+            } else if (k == 1 || m0 == 0) {
                 for (int i = 0; i < k; ++i) DE_TRY(hgram(m0 + i, qb + (int64_t)i * D, vb + (int64_t)i * D));
             } else {
                 // Block form of the same two-pass classical Gram-Schmidt: the
@@ -551,7 +621,7 @@ struct Solver {
                     DE_TRY(update_sub(Q, m0, qb, k, dG, m0));
                     DE_TRY(update_sub(V, m0, vb, k, dG, m0));
                 }
-                for (int i = 0; i < k; ++i) DE_TRY(hgram(i, qb + (int64_t)i * D, vb + (int64_t)i * D, qb, vb));
+                DE_TRY(block_cholqr2(qb, vb, k));
             }
         }
         // solution: V (lanham rhs), rhs(:,1,:) = G^{1/2} (:309-316)
@@ -654,8 +724,7 @@ struct Solver {
             if (ns > 0) {
                 DE_TRY(minus_e(S, AW, W, nev));
                 if (gm.max_inner_iter > 0) DE_TRY(precblock(S, nev));
-                DE_TRY(orth_against(X, nev, S, nev));
-                DE_TRY(orth_against(W, nev, S, nev));
+                DE_TRY(orth_against_all({{X, nev, nullptr}, {W, nev, nullptr}}, S, nev));
                 DE_TRY(cholqr(S, nev));
                 DE_TRY(matblock(S, AS, nev));
                 for (int l = 2; l <= ns; ++l) {
@@ -663,17 +732,13 @@ struct Solver {
                     double2 *sl = col(S, j1), *asl = col(AS, j1);
                     DE_TRY(minus_e(sl, col(AS, j1 - nev), col(S, j1 - nev), nev));
                     if (gm.max_inner_iter > 0) DE_TRY(precblock(sl, nev));
-                    DE_TRY(orth_against(X, nev, sl, nev));
-                    DE_TRY(orth_against(W, nev, sl, nev));
-                    DE_TRY(orth_against(S, j1, sl, nev));
+                    DE_TRY(orth_against_all({{X, nev, nullptr}, {W, nev, nullptr}, {S, j1, nullptr}}, sl, nev));
                     DE_TRY(cholqr(sl, nev));
                     DE_TRY(matblock(sl, asl, nev));
                 }
             }
             if (it > 1) {
-                DE_TRY(orth_against(X, nev, P, nev, AX, AP));
-                DE_TRY(orth_against(W, nev, P, nev, AW, AP));
-                if (ldr > 0) DE_TRY(orth_against(S, ldr, P, nev, AS, AP));
+                DE_TRY(orth_against_all({{X, nev, AX}, {W, nev, AW}, {S, ldr, AS}}, P, nev, AP));
                 DE_TRY(cholqr(P, nev));
                 DE_TRY(trsm(AP, nev));
             }
