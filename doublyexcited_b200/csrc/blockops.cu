@@ -135,14 +135,14 @@ __global__ void __launch_bounds__(256)
             yb[j] = make_double2(0.0, 0.0);
             if (j < nout && (U.beta[j].x != 0.0 || U.beta[j].y != 0.0)) yb[j] = cmul(U.beta[j], ldp(U.y[j] + r));
         }
-        // four input columns a step, their loads issued together
+        // eight input columns a step, their loads issued together
         int i = 0;
-        for (; i + 4 <= nin; i += 4) {
-            double2 xv[4];
+        for (; i + 8 <= nin; i += 8) {
+            double2 xv[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) xv[u] = ldp(U.x[i + u] + r);
+            for (int u = 0; u < 8; ++u) xv[u] = ldp(U.x[i + u] + r);
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
+            for (int u = 0; u < 8; ++u)
 #pragma unroll
                 for (int j = 0; j < NOUT; ++j) {
                     const double2 c = cs[(i + u) * NOUT + j];
@@ -1005,29 +1005,58 @@ __global__ void __launch_bounds__(512)
         for (int b = 0; b < NTW; ++b) re[a][b][0] = re[a][b][1] = im[a][b][0] = im[a][b][1] = 0.0;
     const int64_t r0 = (int64_t)blockIdx.x * chunk;
     const int64_t r1 = min(len, r0 + chunk);
-    for (int64_t rb = r0 + 4 * (int64_t)g; rb < r1; rb += 4 * (int64_t)rg) {
-        const int64_t r = rb + q4;
-        const bool rok = r < r1;
-        double2 lv[MTW], rv[NTW];
+    // The lane's column pointers, read once: indexing the parameter lists
+    // with a lane-dependent column inside the loop would serialise the
+    // constant-cache reads of every load.
+    const S *la[MTW], *lb[MTW], *ra[NTW], *rbp[NTW];
 #pragma unroll
-        for (int a = 0; a < MTW; ++a) {
-            const int i = 8 * (wi * MTW + a) + r8;
-            lv[a] = (rok && i < nl) ? col_elem(L, i, r) : make_double2(0.0, 0.0);
+    for (int a = 0; a < MTW; ++a) {
+        const int i = 8 * (wi * MTW + a) + r8;
+        la[a] = i < nl ? L.a[i] : nullptr;
+        lb[a] = i < nl ? L.b[i] : nullptr;
+    }
+#pragma unroll
+    for (int b = 0; b < NTW; ++b) {
+        const int j = 8 * (wj * NTW + b) + r8;
+        ra[b] = j < nr ? R.a[j] : nullptr;
+        rbp[b] = j < nr ? R.b[j] : nullptr;
+    }
+    auto elem = [](const S *pa, const S *pb, double2 sgm, int64_t r) {
+        double2 v = ld2(pa + r);
+        if (pb) {
+            const double2 w = ld2(pb + r);
+            v.x -= sgm.x * w.x - sgm.y * w.y;
+            v.y -= sgm.x * w.y + sgm.y * w.x;
+        }
+        return v;
+    };
+    // two 4-row steps an iteration for the small warp tiles, their loads
+    // issued first
+    constexpr int US = MTW * NTW >= 4 ? 1 : 2;
+    for (int64_t rb = r0 + 4 * (int64_t)g; rb < r1; rb += 4 * US * (int64_t)rg) {
+        double2 lv[US][MTW], rv[US][NTW];
+#pragma unroll
+        for (int u = 0; u < US; ++u) {
+            const int64_t r = rb + 4 * (int64_t)rg * u + q4;
+            const bool rok = r < r1;
+#pragma unroll
+            for (int a = 0; a < MTW; ++a)
+                lv[u][a] = (rok && la[a]) ? elem(la[a], lb[a], L.sigma, r) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int b = 0; b < NTW; ++b)
+                rv[u][b] = (rok && ra[b]) ? elem(ra[b], rbp[b], R.sigma, r) : make_double2(0.0, 0.0);
         }
 #pragma unroll
-        for (int b = 0; b < NTW; ++b) {
-            const int j = 8 * (wj * NTW + b) + r8;
-            rv[b] = (rok && j < nr) ? col_elem(R, j, r) : make_double2(0.0, 0.0);
-        }
+        for (int u = 0; u < US; ++u)
 #pragma unroll
-        for (int a = 0; a < MTW; ++a)
+            for (int a = 0; a < MTW; ++a)
 #pragma unroll
-            for (int b = 0; b < NTW; ++b) {
-                dmma_g(re[a][b][0], re[a][b][1], lv[a].x, rv[b].x);
-                dmma_g(re[a][b][0], re[a][b][1], lv[a].y, sg * rv[b].y);
-                dmma_g(im[a][b][0], im[a][b][1], lv[a].x, rv[b].y);
-                dmma_g(im[a][b][0], im[a][b][1], lv[a].y, -sg * rv[b].x);
-            }
+                for (int b = 0; b < NTW; ++b) {
+                    dmma_g(re[a][b][0], re[a][b][1], lv[u][a].x, rv[u][b].x);
+                    dmma_g(re[a][b][0], re[a][b][1], lv[u][a].y, sg * rv[u][b].y);
+                    dmma_g(im[a][b][0], im[a][b][1], lv[u][a].x, rv[u][b].y);
+                    dmma_g(im[a][b][0], im[a][b][1], lv[u][a].y, -sg * rv[u][b].x);
+                }
     }
     // sum the row groups in shared memory (fixed order), then one partial per block
     extern __shared__ double2 gtc_sm[];  // [rg][per*32][MTW*NTW*2]
