@@ -114,24 +114,44 @@ int gram_blocks(int nl, int nr, int64_t len)
 
 // ---------------------------------------------------------------- update
 
+// Arithmetic of the block update: FP32 when input and output are both
+// complex64 (the mixed form's inner solve, where the sums run over at most
+// 40 terms and feed a preconditioner), FP64 otherwise.
+template <class SI, class SO>
+struct UpdArith {
+    using T = double;
+    using T2 = double2;
+};
+template <>
+struct UpdArith<float2, float2> {
+    using T = float;
+    using T2 = float2;
+};
+
 template <class SI, class SO, int NOUT>
 __global__ void __launch_bounds__(256)
     update_kernel(const __grid_constant__ UpdListT<SI, SO> U, const double2 *__restrict__ C, int ldc,
                   int64_t len)
 {
-    extern __shared__ double2 cs[];  // [nin][NOUT]
+    using T = typename UpdArith<SI, SO>::T;
+    using T2 = typename UpdArith<SI, SO>::T2;
+    extern __shared__ __align__(16) unsigned char upd_sm[];
+    T2 *cs = reinterpret_cast<T2 *>(upd_sm);  // [nin][NOUT]
     const int nin = U.nin, nout = U.nout;
     for (int idx = threadIdx.x; idx < nin * NOUT; idx += blockDim.x) {
         const int i = idx / NOUT, j = idx % NOUT;
-        cs[idx] = (j < nout) ? C[i + (int64_t)ldc * j] : make_double2(0.0, 0.0);
+        const double2 c = (j < nout) ? C[i + (int64_t)ldc * j] : make_double2(0.0, 0.0);
+        cs[idx].x = (T)c.x;
+        cs[idx].y = (T)c.y;
     }
     __syncthreads();
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
-        double2 acc[NOUT], yb[NOUT];
+        T ar[NOUT], ai[NOUT];
+        double2 yb[NOUT];
 #pragma unroll
         for (int j = 0; j < NOUT; ++j) {
-            acc[j] = make_double2(0.0, 0.0);
+            ar[j] = ai[j] = T(0);
             yb[j] = make_double2(0.0, 0.0);
             if (j < nout && (U.beta[j].x != 0.0 || U.beta[j].y != 0.0)) yb[j] = cmul(U.beta[j], ldp(U.y[j] + r));
         }
@@ -142,31 +162,34 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
             for (int u = 0; u < 8; ++u) xv[u] = ldp(U.x[i + u] + r);
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
+            for (int u = 0; u < 8; ++u) {
+                const T xr = (T)xv[u].x, xi = (T)xv[u].y;
 #pragma unroll
                 for (int j = 0; j < NOUT; ++j) {
-                    const double2 c = cs[(i + u) * NOUT + j];
-                    acc[j].x = fma(xv[u].x, c.x, acc[j].x);
-                    acc[j].x = fma(-xv[u].y, c.y, acc[j].x);
-                    acc[j].y = fma(xv[u].x, c.y, acc[j].y);
-                    acc[j].y = fma(xv[u].y, c.x, acc[j].y);
+                    const T2 c = cs[(i + u) * NOUT + j];
+                    ar[j] = fma(xr, c.x, ar[j]);
+                    ar[j] = fma(-xi, c.y, ar[j]);
+                    ai[j] = fma(xr, c.y, ai[j]);
+                    ai[j] = fma(xi, c.x, ai[j]);
                 }
+            }
         }
         for (; i < nin; ++i) {
             const double2 xv = ldp(U.x[i] + r);
+            const T xr = (T)xv.x, xi = (T)xv.y;
 #pragma unroll
             for (int j = 0; j < NOUT; ++j) {
-                const double2 c = cs[i * NOUT + j];
-                acc[j].x = fma(xv.x, c.x, acc[j].x);
-                acc[j].x = fma(-xv.y, c.y, acc[j].x);
-                acc[j].y = fma(xv.x, c.y, acc[j].y);
-                acc[j].y = fma(xv.y, c.x, acc[j].y);
+                const T2 c = cs[i * NOUT + j];
+                ar[j] = fma(xr, c.x, ar[j]);
+                ar[j] = fma(-xi, c.y, ar[j]);
+                ai[j] = fma(xr, c.y, ai[j]);
+                ai[j] = fma(xi, c.x, ai[j]);
             }
         }
 #pragma unroll
         for (int j = 0; j < NOUT; ++j) {
-            const double2 s = cmul(U.alpha, acc[j]);
-            if (j < nout) U.y[j][r] = st2<SO>(yb[j].x + s.x, yb[j].y + s.y);
+            const double2 sj = cmul(U.alpha, make_double2((double)ar[j], (double)ai[j]));
+            if (j < nout) U.y[j][r] = st2<SO>(yb[j].x + sj.x, yb[j].y + sj.y);
         }
     }
 }
@@ -174,7 +197,7 @@ __global__ void __launch_bounds__(256)
 template <int NOUT, class SI, class SO>
 cudaError_t update_go(const UpdListT<SI, SO> &U, const double2 *c, int ldc, int64_t len, cudaStream_t st)
 {
-    const size_t smem = (size_t)U.nin * NOUT * sizeof(double2);
+    const size_t smem = (size_t)U.nin * NOUT * sizeof(typename UpdArith<SI, SO>::T2);
     const int64_t want = (len + 255) / 256;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, 148 * 8));
     update_kernel<SI, SO, NOUT><<<blocks, 256, smem, st>>>(U, c, ldc, len);
