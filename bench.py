@@ -262,6 +262,22 @@ def cpu_matvec_seconds(w, reps):
     return (time.perf_counter() - t0) / reps, os.cpu_count()
 
 
+def max_over_ranks(x, dist, device):
+    """The slowest rank's time: every rank contributes its own and all get
+    the maximum (replica timing; no data-path collective)."""
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank, world, seconds):
+    """Whole-job throughput of N independent replicas timed as the max over
+    ranks: all ranks' units over the slowest rank's time."""
+    return units_per_rank * world / seconds
+
+
 def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -570,13 +586,11 @@ def main():
         prof32 = prob.profile_read32()
         prob.set_profiling(False)
         if pg:
-            t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            elapsed = float(t.item())
+            elapsed = max_over_ranks(elapsed, pg, "cuda")
         out = {"prob": prob, "x0": x0, "dim": dim, "elapsed": elapsed, "stats": stats, "st": stats[-1],
                "e": complex(e_host[0]), "e_all": e_host.copy(), "prof": prof, "prof32": prof32,
                "launches": launches,
-               "clocks": clocks, "value": a.steps * world / elapsed}
+               "clocks": clocks, "value": replica_rate(a.steps, world, elapsed)}
         del x_dev, x0_dev
         return out
 
@@ -612,10 +626,8 @@ def main():
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
     if pg:
-        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_e2e = float(t.item())
-    e2e = e2e_steps * world / t_e2e
+        t_e2e = max_over_ranks(t_e2e, pg, "cuda")
+    e2e = replica_rate(e2e_steps, world, t_e2e)
 
     peak = fp64_peak_tflops(torch)
     peak32 = fp32_peak_tflops(torch)
