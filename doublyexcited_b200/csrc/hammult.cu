@@ -329,11 +329,13 @@ cudaError_t launch_cube(const HamDev &h, const CubeArgs<R> &a, int64_t ncubes, c
 //   * after a barrier the owner adds the group's line outputs to its outputs.
 // Two barriers per group of G slabs.
 
-template <int NN>
+template <int NN, class R = double>
 struct SCfg {
     static constexpr int M = NN * NN * NN;
     static constexpr int P2 = NN * NN;
-    static constexpr int G = NN == 13 ? 3 : NN == 15 ? 4 : NN == 17 ? 4 : 5;  // slabs per group
+    // slabs per group; complex64 at NN=13 takes larger groups (fewer
+    // barriers per cube; shared memory is no limit there)
+    static constexpr int G = (NN == 13 && sizeof(R) == 4) ? 5 : NN == 13 ? 3 : NN == 15 ? 4 : NN == 17 ? 4 : 5;
     static constexpr int CSZ = (NN + 1) / 2;                                   // outputs per chunk
     static constexpr int WPC = (2 * NN * G + 31) / 32;                         // warps per chunk
     static constexpr int NT_LINES = 2 * WPC * 32;
@@ -342,12 +344,15 @@ struct SCfg {
     static constexpr int NG = (NN + G - 1) / G;  // groups per cube
     static constexpr int MINB = NT <= 256 ? 2 : 1;
 };
-// complex64 storage needs fewer registers: one more resident CTA per SM (a
-// fourth one at NN=13 fits without spills but measured no faster)
+// resident CTAs per SM the launch bounds ask for: complex64 storage needs
+// fewer registers, so one more CTA (a fourth at NN=13 fits without spills
+// but measured no faster), and two of the 320-thread complex64 NN=13 CTAs
 template <int NN, class R>
 constexpr int smin_blocks()
 {
-    return SCfg<NN>::MINB + ((sizeof(R) == 4 && SCfg<NN>::NT <= 256) ? 1 : 0);
+    using C = SCfg<NN, R>;
+    if constexpr (sizeof(R) == 4) return C::NT <= 256 ? C::MINB + 1 : 2;
+    return C::MINB;
 }
 
 // Asynchronous global -> shared copy of one complex element (16 bytes for
@@ -372,7 +377,7 @@ __device__ __forceinline__ void cp_wait()
 template <class R, int NN, int MODE>
 __device__ __forceinline__ void issue_group(const CubeArgs<R> &a, int64_t cube, int g, C2<R> *ring, int half)
 {
-    using C = SCfg<NN>;
+    using C = SCfg<NN, R>;
     constexpr int P2 = C::P2, M = C::M, G = C::G;
     const int64_t vec = cube / M, c = cube - vec * M;
     const C2<R> *xv = a.x + vec * a.vstride;
@@ -390,7 +395,7 @@ __device__ __forceinline__ void issue_group(const CubeArgs<R> &a, int64_t cube, 
 template <class R, int NN, int CK>
 __device__ __forceinline__ void line_chunk2(const HamDev &h, const C2<R> *xs, int xs_stride, C2<R> *u, int u_stride)
 {
-    constexpr int CSZ = SCfg<NN>::CSZ;
+    constexpr int CSZ = SCfg<NN, R>::CSZ;
     constexpr int O0 = CK * CSZ;
     constexpr int O1 = (O0 + CSZ < NN) ? O0 + CSZ : NN;
     constexpr int NO = O1 - O0;
@@ -416,7 +421,7 @@ __device__ __forceinline__ void stream_groups(const HamDev &h, const CubeArgs<R>
                                               C2<R> *ring, C2<R> *ub, int &half, R (&ar)[NN], R (&ai)[NN], int ip,
                                               int jp, int kp, R t1p)
 {
-    using C = SCfg<NN>;
+    using C = SCfg<NN, R>;
     constexpr int P2 = C::P2, G = C::G, NG = C::NG, WPC = C::WPC;
     if constexpr (GI < NG) {
         constexpr int L0 = GI * G;
@@ -507,10 +512,10 @@ __device__ __forceinline__ void stream_groups(const HamDev &h, const CubeArgs<R>
 }
 
 template <class R, int NN, int MODE>
-__global__ void __launch_bounds__(SCfg<NN>::NT, (smin_blocks<NN, R>()))
+__global__ void __launch_bounds__(SCfg<NN, R>::NT, (smin_blocks<NN, R>()))
     stream_kernel(const __grid_constant__ HamDev h, const __grid_constant__ CubeArgs<R> a, int64_t ncubes)
 {
-    using C = SCfg<NN>;
+    using C = SCfg<NN, R>;
     constexpr int P2 = C::P2, M = C::M;
     extern __shared__ __align__(16) unsigned char ssm_raw[];
     C2<R> *ring = reinterpret_cast<C2<R> *>(ssm_raw);  // [2][G][P2]
@@ -572,7 +577,7 @@ int sm_count()
 template <class R, int NN, int MODE>
 cudaError_t launch_stream(const HamDev &h, const CubeArgs<R> &a, int64_t ncubes, cudaStream_t st)
 {
-    using C = SCfg<NN>;
+    using C = SCfg<NN, R>;
     const size_t smem = (size_t)4 * C::G * C::P2 * sizeof(C2<R>);
     static bool attr[64] = {};
     int dev = 0;
