@@ -351,7 +351,7 @@ template <int NN, class R>
 constexpr int smin_blocks()
 {
     using C = SCfg<NN, R>;
-    if constexpr (sizeof(R) == 4) return C::NT <= 256 ? C::MINB + 1 : 2;
+    if constexpr (sizeof(R) == 4) return C::NT <= 256 ? C::MINB + 1 : NN == 13 ? 2 : C::MINB;
     return C::MINB;
 }
 
