@@ -153,7 +153,7 @@ def alg_bytes(nn):
 # dram bytes (read + write) per vector-matvec (pass A + pass B), keyed by
 # (NN, storage), from the ncu capture of the block-of-2 matvec at N=6
 # (profiles/stream_kernel_matvec-n6.md): both passes' bytes over 2 vectors.
-NCU_TRAFFIC_PER_VECTOR = {(13, "f64"): 343.25e6, (13, "f32"): 151.75e6}
+NCU_TRAFFIC_PER_VECTOR = {(13, "f64"): 342.25e6, (13, "f32"): 151.8e6}
 
 
 class ClockSampler:
