@@ -187,3 +187,31 @@ def test_dots_shapes(de, nb, nk):
         c = g.dots(a, b, hermitian=False)
     assert np.max(np.abs(h - a.conj().T @ b)) < 1e-9
     assert np.max(np.abs(c - a.T @ b)) < 1e-9
+
+
+def test_trim_releases_workspace_and_solves_again(de, oracle):
+    """de_problem_trim gives the cached workspace back; the next solve
+    allocates it again and reproduces the same bits."""
+    p = oracle.Params(n=3, delta=2.0, theta=0.3)
+    x0 = oracle.seeded_start(p, 1, 3)
+    with de.Problem(n=3, delta=2.0, theta=0.3) as h:
+        r1 = h.gplmr_eig(x0, -0.78, maxit=5, tol=1e-14)
+        de.lib().de_problem_trim(h.handle)
+        r2 = h.gplmr_eig(x0, -0.78, maxit=5, tol=1e-14)
+    assert r1.e[0] == r2.e[0]
+
+
+def test_mixed_profiling_counts_fp32_products(de, oracle):
+    """The mixed form's inner-solve matvecs are timed apart from the FP64
+    MATBLOCKs (de_profile_read32): 5 FP32 products per PRECBLOCK call at
+    order 5 and NEV = 1, one FP64 product per MATBLOCK."""
+    p = oracle.Params(n=3, delta=2.0, theta=0.3)
+    x0 = oracle.seeded_start(p, 1, 3)
+    with de.Problem(n=3, delta=2.0, theta=0.3, precision="mixed") as h:
+        h.set_profiling(True)
+        r = h.gplmr_eig(x0, -0.78, maxit=2, tol=1e-14)
+        p64, p32 = h.profile_read(), h.profile_read32()
+    assert r.iterations == 2
+    assert p64["vectors"] == 1 + 2 * 6          # start + (1 + NS) blocks per iteration
+    assert p32["vectors"] == 2 * 6 * 5          # (1 + NS) PRECBLOCK calls x 5 products
+    assert p32["pass_a_ms"] > 0 and p32["pass_b_ms"] > 0
