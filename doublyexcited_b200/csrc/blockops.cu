@@ -10,9 +10,11 @@
 // are bitwise identical.
 //
 // Every kernel here streams its vectors once; they are HBM-bound except the
-// 64 x 64 projection Gram, which is FP64-FMA bound (8 flops per complex MAC).
+// 64 x 128 projection Gram, which runs on the FP64 tensor cores (gram_tc).
 // The vector kernels are templated on the storage type S (double2, or
-// float2 for the mixed form's inner solve); sums always accumulate in FP64.
+// float2 for the mixed form's inner solve); reductions accumulate in FP64,
+// and only the complex64 block update (a preconditioner's combination of at
+// most 40 columns) computes in FP32.
 #include "de_internal.h"
 #include "de_kernels.h"
 
@@ -1151,7 +1153,7 @@ static cudaError_t gram_tc_go(const ColListT<S> &L, const ColListT<S> &R, int64_
         attr[dev] = true;
     }
     // about four blocks per SM; the partials (nblk x nl x nr) fit the work
-    // buffer that gram_work_elems sizes for the tiled path
+    // buffer that gram_work_elems sizes for them
     const int nblk = gram_blocks(L.n, R.n, len);
     int64_t chunk = (len + nblk - 1) / nblk;
     chunk = (chunk + 3) / 4 * 4;
