@@ -586,15 +586,19 @@ def main():
         torch.cuda.synchronize()
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
         launches0 = L.de_kernel_launches()
         e0.record(stream)
         stats = []
-        for _ in range(a.steps):
+        for i in range(a.steps):
+            marks[i].record(stream)
             stats.append(solve_dev())
+        marks[a.steps].record(stream)
         e1.record(stream)
         launches = L.de_kernel_launches() - launches0
         torch.cuda.synchronize()
         elapsed = e0.elapsed_time(e1) / 1e3
+        per_solve = [marks[i].elapsed_time(marks[i + 1]) / 1e3 for i in range(a.steps)]
         barrier()
         clocks = sampler.stop() if sampler else None
         prof = prob.profile_read()
@@ -604,7 +608,7 @@ def main():
             elapsed = max_over_ranks(elapsed, pg, "cuda")
         out = {"prob": prob, "x0": x0, "dim": dim, "elapsed": elapsed, "stats": stats, "st": stats[-1],
                "e": complex(e_host[0]), "e_all": e_host.copy(), "prof": prof, "prof32": prof32,
-               "launches": launches,
+               "launches": launches, "per_solve": per_solve,
                "clocks": clocks, "value": replica_rate(a.steps, world, elapsed)}
         del x_dev, x0_dev
         return out
@@ -620,6 +624,9 @@ def main():
     elapsed, st, e_final, prof, launches, clocks = (head["elapsed"], head["st"], head["e"], head["prof"],
                                                      head["launches"], head["clocks"])
     value = head["value"]
+    lat = np.array(head["per_solve"])
+    latency = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+               "solves": len(lat), "note": "device time per solve, one solve at a time"}
     e_host = np.empty(w["nev"], np.complex128)
 
     # end to end through the host-pointer C ABI (pinned host buffers)
@@ -683,7 +690,9 @@ def main():
     compare = {"fp64_error": other_err} if other_err else None
     if other is not None:
         de_max = float(np.max(np.abs(np.sort_complex(head["e_all"]) - np.sort_complex(other["e_all"]))))
+        olat = np.array(other["per_solve"])
         compare = {"fp64_value": other["value"], "fp64_ms_per_step": other["elapsed"] / a.steps * 1e3,
+                   "fp64_p50_s": float(np.percentile(olat, 50)), "fp64_p99_s": float(np.percentile(olat, 99)),
                    "fp64_iterations": other["st"].iterations, "fp64_E": [other["e"].real, other["e"].imag],
                    "speedup_vs_fp64": value / other["value"], "dE_vs_fp64": de_max}
         other["prob"].close()
@@ -706,6 +715,7 @@ def main():
             "roofline": roofline,
             "roofline_other_matvec": roofline_other,
             "cpu_baseline": cpu,
+            "latency": latency,
             "mixed_vs_fp64": compare,
             "gpu_launches": int(launches),
             "clocks": clocks,
