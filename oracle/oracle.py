@@ -22,7 +22,10 @@ It restates, loop for loop where it matters, the Fortran reference
   ``fast_harmritz_setup``/``myhgramschmidt_many``
   harmonic_ritz_small.F90:28-324 and ``gen_cmatsub`` hr_eigen.f90:223-291;
 * ``GET_EXPECTS`` hammod.F90:1261-1301 and the shift rule
-  doublyexcited.F90:214-219.
+  doublyexcited.F90:214-219;
+* the initial guess: He+ orbitals (dense, where the reference runs block
+  Lanczos), ``HELIUM_ORBITALGATHER`` / ``HELIUM_ORBITAL`` /
+  ``DIAGSUBSPACE`` / ``mysort`` hammod.F90:1041-1256,1658-1690.
 
 Dense LAPACK calls go to the same routines the reference calls (``dsyev``,
 ``zggev``, ``zgesdd``, ``zpotrf``, ``ztrsm``) through scipy's LAPACK.
@@ -538,6 +541,83 @@ def gplmr_shift(expects: np.ndarray, nev: int, takerealpart: bool = True) -> com
     """doublyexcited.F90:214-219."""
     s = complex(np.sum(expects[:nev]) / nev)
     return complex(s.real, 0.0) if takerealpart else s
+
+
+# --------------------------------------------------------------------------
+# initial guess: He+ orbitals, product states, subspace diagonalisation
+
+
+def heplus_orbitals(h1: Hamiltonian, numorbs: int):
+    """The numorbs He+ levels of lowest real part and their right
+    eigenvectors.  The reference converges them with block Lanczos
+    (lanmod.F90, called from doublyexcited.F90:135-137); here a dense
+    ZGEEV (np.linalg.eig) of the same operator."""
+    w, v = np.linalg.eig(dense_one_electron(h1))
+    idx = np.argsort(w.real, kind="stable")[:numorbs]
+    return w[idx], np.asfortranarray(v[:, idx])
+
+
+def orbital_gather(x: np.ndarray, hermopt: bool = False) -> np.ndarray:
+    """The Gram-Schmidt of HELIUM_ORBITALGATHER hammod.F90:1084-1113:
+    c-products (or Hermitian products with hermopt), modified, in order."""
+    x = np.array(x, dtype=np.complex128, order="F", copy=True)
+    dot = (lambda a, b: np.vdot(a, b)) if hermopt else (lambda a, b: np.dot(a, b))
+    for i in range(x.shape[1]):
+        for j in range(i):
+            x[:, i] -= x[:, j] * dot(x[:, j], x[:, i])
+        x[:, i] /= np.sqrt(dot(x[:, i], x[:, i]))
+    return x
+
+
+def helium_orbital(ev: np.ndarray, i: int, j: int, sign: int) -> np.ndarray:
+    """HELIUM_ORBITAL hammod.F90:1041-1080: PSI(p,q) = X_i(p) X_j(q) +
+    sign X_j(p) X_i(q), halved when i == j, else divided by sqrt(2);
+    electron 1 (p) fastest."""
+    a, b = ev[:, i], ev[:, j]
+    psi = np.outer(a, b) + sign * np.outer(b, a)  # psi[p, q]
+    psi = psi.reshape(-1, order="F")
+    return psi / 2.0 if i == j else psi / math.sqrt(2.0)
+
+
+def mysort_order(values: np.ndarray, etarget: complex) -> list:
+    """mysort hammod.F90:1658-1690: repeatedly the untaken value nearest
+    etarget; among equal distances the later index wins (.le.)."""
+    n = len(values)
+    taken = [False] * n
+    order = []
+    for _ in range(n):
+        best, low = -1, None
+        for i in range(n):
+            if not taken[i]:
+                d = abs(values[i] - etarget)
+                if best < 0 or d <= low:
+                    best, low = i, d
+        taken[best] = True
+        order.append(best)
+    return order
+
+
+def diagsubspace(h2: Hamiltonian, ev: np.ndarray, singlet: bool, hermopt: bool, etarget: complex,
+                 numout: int):
+    """DIAGSUBSPACE hammod.F90:1125-1256: H in the span of the symmetrised
+    products of the orbitals (i <= j for singlets, i < j for triplets),
+    ZGEEV of A(I,J) = psi_I . (H psi_J), eigenvalues ordered by distance to
+    etarget (mysort), the first numout eigenvectors as two-electron vectors
+    with unit Hermitian norm."""
+    numorbs = ev.shape[1]
+    sign = 1 if singlet else -1
+    table = [(i, j) for i in range(numorbs) for j in range(i + (0 if singlet else 1), numorbs)]
+    psi = np.empty((h2.dim, len(table)), np.complex128, order="F")
+    for k, (i, j) in enumerate(table):
+        psi[:, k] = helium_orbital(ev, i, j, sign)
+    hpsi = h2.matblock(psi)
+    a = (psi.conj().T @ hpsi) if hermopt else (psi.T @ hpsi)
+    e0, vr = np.linalg.eig(a)
+    order = mysort_order(e0, etarget)
+    e0, vr = e0[order], vr[:, order]
+    out = np.asfortranarray(psi @ vr[:, :numout])
+    out /= np.sqrt(np.einsum("ij,ij->j", out.conj(), out).real)
+    return e0[:numout], out, e0
 
 
 # --------------------------------------------------------------------------

@@ -109,3 +109,32 @@ def test_oracle_gplmr_small_runs(oracle):
     assert r.iterations == 4
     assert r.matvecs == 1 + 4 * 6 * (1 + 11)
     assert r.history[-1][2][0] < r.history[0][2][0]
+
+
+def test_subspace_guess_matches_reference_log(oracle):
+    """The initial guess at N=5 (14 He+ orbitals, singlet products, c-product
+    subspace): the six subspace eigenvalues nearest the shift equal those the
+    reference printed (Out.S.N5:100-107) to the accuracy of its Lanczos
+    orbitals (error 1.8e-3 at Out.S.N5:48).  With exact orbitals the 2p-like
+    triple is exactly degenerate; the reference's is split by ~1e-5."""
+    p = oracle.Params(n=5, delta=2.0, theta=0.2)
+    h1 = oracle.init_hamiltonian(p, nelec=1)
+    h2 = oracle.init_hamiltonian(p, nelec=2)
+    _, v = oracle.heplus_orbitals(h1, 14)
+    ev = oracle.orbital_gather(v)
+    e0, x, _ = oracle.diagsubspace(h2, ev, True, False, -0.7131541429, 6)
+    log = [(-0.70668286560422, 0.03676471730071), (-0.63390932605588, 0.02889602525833),
+           (-0.63390456155722, 0.02890205309617), (-0.63390250056812, 0.02890988095510),
+           (-0.63028124855576, 0.02597489130175), (-0.63027701879070, 0.02598683463795)]
+    log = np.array([complex(a, b) for a, b in log])
+    assert abs(e0[0] - log[0]) < 5e-6
+    assert np.max(np.abs(e0 - log)) < 2e-5
+    # the guess vectors: unit Hermitian norm, singlet (X = X^T), and their
+    # Rayleigh quotients are the subspace eigenvalues (H is diagonal there)
+    m = p.m
+    for j in range(6):
+        assert abs(np.linalg.norm(x[:, j]) - 1.0) < 1e-12
+        xm = x[:, j].reshape(m, m, order="F")
+        assert np.max(np.abs(xm - xm.T)) < 1e-12
+    hx = h2.matvec(x[:, 0])
+    assert abs(np.dot(x[:, 0], hx) / np.dot(x[:, 0], x[:, 0]) - e0[0]) < 1e-10
