@@ -163,6 +163,8 @@ SIGNATURES = {
     "de_dots_d": (INT, [P, P, P, I64, INT, INT, P, INT]),
     "de_dots_noalloc_d": (INT, [P, P, I64, INT, INT, P, INT, P]),
     "de_get_expects": (INT, [P, P, INT, INT, P]),
+    "de_subspace_guess": (INT, [P, INT, INT, INT, de_complex, INT, P, P]),
+    "de_subspace_guess_d": (INT, [P, INT, INT, INT, de_complex, INT, P, P]),
     "de_gplmr_eig": (INT, [P, P, P, I64, I64, de_complex, INT, INT, INT, ctypes.c_double,
                            ctypes.POINTER(de_gmres), INT, ctypes.POINTER(de_stats)]),
     "de_gplmr_eig_d": (INT, [P, P, P, I64, I64, de_complex, INT, INT, INT, ctypes.c_double,

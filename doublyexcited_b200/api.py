@@ -166,6 +166,17 @@ class Problem:
               "de_get_expects")
         return out
 
+    def subspace_guess(self, numorbs: int, singlet: bool = True, hermopt: bool = False,
+                       etarget: complex = 0.0, numout: int = 1) -> tuple[np.ndarray, np.ndarray]:
+        """The reference's GPLMR start block: (E0[:numout], X (D, numout))."""
+        x = np.empty((self.dim, numout), np.complex128, order="F")
+        e0 = np.empty(numout, np.complex128)
+        et = complex(etarget)
+        check(lib().de_subspace_guess(self._h, numorbs, int(bool(singlet)), int(bool(hermopt)),
+                                      de_complex(et.real, et.imag), numout, _ptr(x), _ptr(e0)),
+              "de_subspace_guess")
+        return e0, x
+
     # -- eigensolver ----------------------------------------------------------
     def gplmr_eig(self, x0: np.ndarray, sigma: complex, ns: int = 5, maxit: int = 100, tol: float = 1e-7,
                   max_inner_iter: int = 5, usepetscflag: int = 1, compat_first_column_only: bool = False,

@@ -42,6 +42,8 @@ struct Lapack {
     void (*zgesdd)(const char *, const int *, const int *, cplx *, const int *, double *, cplx *,
                    const int *, cplx *, const int *, cplx *, const int *, double *, int *, int *,
                    size_t) = nullptr;
+    void (*zgeev)(const char *, const char *, const int *, cplx *, const int *, cplx *, cplx *, const int *,
+                  cplx *, const int *, cplx *, const int *, double *, int *, size_t, size_t) = nullptr;
 };
 const Lapack &lapack();  // loads once; check .ok
 

@@ -58,11 +58,12 @@ static Lapack load_lapack()
                 std::string s = std::string(pre) + name;
                 return dlsym(hd, s.c_str());
             };
-            void *a = sym("zggev_"), *b = sym("zpotrf_"), *d = sym("zgesdd_");
-            if (a && b && d) {
+            void *a = sym("zggev_"), *b = sym("zpotrf_"), *d = sym("zgesdd_"), *g = sym("zgeev_");
+            if (a && b && d && g) {
                 L.zggev = reinterpret_cast<decltype(L.zggev)>(a);
                 L.zpotrf = reinterpret_cast<decltype(L.zpotrf)>(b);
                 L.zgesdd = reinterpret_cast<decltype(L.zgesdd)>(d);
+                L.zgeev = reinterpret_cast<decltype(L.zgeev)>(g);
                 L.ok = true;
                 L.path = c;
                 return L;

@@ -208,6 +208,28 @@ DE_API int de_dots_noalloc_d(const de_complex *bras_d, const de_complex *kets_d,
 DE_API int de_get_expects(de_problem *h, const de_complex *psi, int nvec, int cshiftopt,
                           de_complex *expects);
 
+/* ---- initial guess: HELIUM_ORBITAL products + DIAGSUBSPACE ---------- */
+
+/* The reference's start block for GPLMR (doublyexcited.F90:135-190).
+ * The numorbs He+ levels of lowest real part come from the one-electron
+ * operator of the handle's grid.  The reference converges them with block
+ * Lanczos; here a dense ZGEEV is used, so numorbs <= M.  They are
+ * Gram-Schmidt orthonormalised as in HELIUM_ORBITALGATHER
+ * hammod.F90:1084-1113: c-products, or Hermitian products with hermopt.
+ * The symmetrised products HELIUM_ORBITAL hammod.F90:1041-1080 follow
+ * (i <= j for singlet, i < j otherwise).  H is diagonalised in their span,
+ * as in DIAGSUBSPACE hammod.F90:1125-1256: A(I,J) = psi_I . H psi_J, ZGEEV,
+ * then eigenvalues ordered by distance to etarget as in mysort
+ * hammod.F90:1658-1690.  Outputs: the first numout eigenvalues in e0, and
+ * the two-electron vectors in x (D x numout, column-major, unit Hermitian
+ * norm).  At most 128 products and 16 outputs; numout above the number of
+ * products returns DE_E_INVALID (the reference STOPs with "Reset NUMOUT").
+ * _d: x is device memory.  Needs a nelec == 2 handle and host LAPACK. */
+DE_API int de_subspace_guess_d(de_problem *h, int numorbs, int singlet, int hermopt, de_complex etarget,
+                               int numout, de_complex *x_d, de_complex *e0);
+DE_API int de_subspace_guess(de_problem *h, int numorbs, int singlet, int hermopt, de_complex etarget,
+                             int numout, de_complex *x, de_complex *e0);
+
 /* ---- eigensolver: GPLMR_EIG ----------------------------------------- */
 
 /* Block GPLMR with harmonic projection and the BASIC inner solve.
