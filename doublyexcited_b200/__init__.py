@@ -12,6 +12,9 @@ mirroring the reference's entry points (paths relative to
 * :meth:`Problem.dots`      -- ``MYDOTSUB`` doublyexcited.F90:47-59 / ``MPIDOT``
 * :meth:`Problem.get_expects` -- ``GET_EXPECTS`` hammod.F90:1261-1301
 * :meth:`Problem.gplmr_eig` -- ``GPLMR_EIG`` gplmr.F90:9-374
+* :meth:`Problem.subspace_guess` -- the initial guess, doublyexcited.F90:135-190
+  (``DIAGSUBSPACE`` hammod.F90:1125-1256), and :func:`heplus_orbitals`, its
+  He+ orbital step on the host
 * :func:`read_input`        -- ``get_input``/``get_args`` input.F90:143-362
 * :func:`write_vectors` / :func:`read_vectors` -- utils.F90:82-198
 * :class:`Server` -- many independent solves on one GPU (no reference
@@ -41,13 +44,14 @@ from ._lib import (  # noqa: F401
     lib,
     lib_path,
 )
-from .api import Problem, GplmrResult, Server, ServedResult, read_input, read_vectors, vectors_header, write_vectors  # noqa: F401,E501
+from .api import Problem, GplmrResult, Server, ServedResult, heplus_orbitals, read_input, read_vectors, vectors_header, write_vectors  # noqa: F401,E501
 
 __all__ = [
     "Problem",
     "GplmrResult",
     "Server",
     "ServedResult",
+    "heplus_orbitals",
     "read_input",
     "read_vectors",
     "vectors_header",

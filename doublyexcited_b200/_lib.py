@@ -165,6 +165,7 @@ SIGNATURES = {
     "de_get_expects": (INT, [P, P, INT, INT, P]),
     "de_subspace_guess": (INT, [P, INT, INT, INT, de_complex, INT, P, P]),
     "de_subspace_guess_d": (INT, [P, INT, INT, INT, de_complex, INT, P, P]),
+    "de_heplus_orbitals": (INT, [INT, P, INT, INT, P, P]),
     "de_gplmr_eig": (INT, [P, P, P, I64, I64, de_complex, INT, INT, INT, ctypes.c_double,
                            ctypes.POINTER(de_gmres), INT, ctypes.POINTER(de_stats)]),
     "de_gplmr_eig_d": (INT, [P, P, P, I64, I64, de_complex, INT, INT, INT, ctypes.c_double,

@@ -195,6 +195,22 @@ class Problem:
 
 # -- configuration ---------------------------------------------------------------
 
+def heplus_orbitals(n: int, h1: np.ndarray, numorbs: int, hermopt: bool = False) -> tuple[np.ndarray, np.ndarray]:
+    """He+ levels of lowest real part and their Gram-Schmidt orthonormalised
+    orbitals from a dense one-electron operator (DIAGONALIZE +
+    HELIUM_ORBITALGATHER); host only.  Returns (energies, orbitals (M, numorbs))."""
+    nn = 2 * n + 1
+    m = nn ** 3
+    h1 = np.asfortranarray(h1, dtype=np.complex128)
+    if h1.shape != (m, m):
+        raise ValueError(f"h1 has shape {h1.shape}, expected ({m}, {m})")
+    w = np.empty(numorbs, np.complex128)
+    orb = np.empty((m, numorbs), np.complex128, order="F")
+    check(lib().de_heplus_orbitals(n, _ptr(h1), numorbs, int(bool(hermopt)), _ptr(w), _ptr(orb)),
+          "de_heplus_orbitals")
+    return w, orb
+
+
 def read_input(path: str | None, argv: list[str] | None = None) -> dict:
     """Input.Inp namelists + command-line keys (get_input / get_args)."""
     L = lib()

@@ -3,15 +3,14 @@
 // span (doublyexcited.F90:135-190; HELIUM_ORBITALGATHER, HELIUM_ORBITAL,
 // DIAGSUBSPACE and mysort hammod.F90:1041-1256,1658-1690).
 //
-// The reference converges the He+ orbitals with block Lanczos (lanmod.F90);
-// here they come from a dense ZGEEV of the one-electron operator, which is
-// built column by column on the GPU (M <= 12167 points).  Products, H times
-// products and the subspace matrix are formed on the device; the k x k
-// eigenproblems run on the host.
+// The reference converges the He+ orbitals with block Lanczos (lanmod.F90).
+// Here they are exact eigenvectors of the one-electron operator: the GPU
+// builds it column by column (M <= 12167 points) and the host runs a ZGEEV
+// per parity sector.  The products, H times the products and the subspace
+// matrix are formed on the device; the k x k eigenproblem runs on the host.
 #include <algorithm>
 #include <cmath>
 #include <memory>
-#include <numeric>
 #include <vector>
 
 #include "de_internal.h"
@@ -94,7 +93,150 @@ struct Handle1 {
     }
 };
 
+// One axis's parity functions about the centre c = (nn-1)/2: even ones are
+// e_c and (e_{c+a} + e_{c-a})/sqrt(2), odd ones (e_{c+a} - e_{c-a})/sqrt(2),
+// a = 1..c.  (i1 < 0: a single point.)
+struct AxisFn {
+    int i0, i1;
+    double w0, w1;
+};
+
+std::vector<AxisFn> axis_basis(int nn, int odd)
+{
+    const int c = (nn - 1) / 2;
+    const double r = 1.0 / std::sqrt(2.0);
+    std::vector<AxisFn> b;
+    if (!odd) b.push_back({c, -1, 1.0, 0.0});
+    for (int a = 1; a <= c; ++a) b.push_back({c + a, c - a, r, odd ? -r : r});
+    return b;
+}
+
 }  // namespace
+
+namespace de {
+
+// The numorbs He+ levels of lowest real part and their right eigenvectors,
+// Gram-Schmidt orthonormalised as HELIUM_ORBITALGATHER hammod.F90:1084-1113
+// does (c-products, or Hermitian products with hermopt), from the dense
+// one-electron operator h1 (M x M, column-major, M = nn^3).
+//
+// The reference converges these levels with block Lanczos (lanmod.F90).
+// Here they are exact eigenvectors.  The operator on the cube commutes with
+// the reflections of each axis about the nucleus, so it is block diagonal in
+// the 8 parity sectors (even/odd along x, y, z), each about M/8 wide; one
+// ZGEEV per sector replaces a ZGEEV of the whole operator (about 64 times
+// fewer flops).  Levels of equal real part keep sector order.
+int heplus_orbitals(int nn, const cplx *h1, int numorbs, int hermopt, std::vector<cplx> &energy,
+                    std::vector<cplx> &orb)
+{
+    const int64_t m = (int64_t)nn * nn * nn;
+    if (nn < 1 || nn % 2 == 0) return set_error(DE_E_INVALID, "grid width %d is not 2N+1", nn);
+    if (numorbs < 1 || numorbs > m)
+        return set_error(DE_E_INVALID, "numorbs %d is not in 1..%lld", numorbs, (long long)m);
+    struct Level {
+        cplx w;
+        int sector, col;
+    };
+    std::vector<Level> levels;
+    std::vector<std::vector<cplx>> vecs(8);
+    std::vector<std::vector<int>> sup_idx(8);
+    std::vector<std::vector<double>> sup_w(8);
+    std::vector<int> dims(8);
+    for (int sec = 0; sec < 8; ++sec) {
+        const auto bx = axis_basis(nn, sec & 1), by = axis_basis(nn, (sec >> 1) & 1), bz = axis_basis(nn, (sec >> 2) & 1);
+        const int ds = (int)(bx.size() * by.size() * bz.size());
+        dims[sec] = ds;
+        if (ds == 0) continue;
+        // support of each sector function: up to 8 grid points and weights
+        std::vector<int> &si = sup_idx[sec];
+        std::vector<double> &sw = sup_w[sec];
+        si.assign((size_t)ds * 8, -1);
+        sw.assign((size_t)ds * 8, 0.0);
+        int k = 0;
+        for (const auto &fz : bz)
+            for (const auto &fy : by)
+                for (const auto &fx : bx) {
+                    int t = 0;
+                    for (int cz = 0; cz < 2; ++cz) {
+                        const int iz = cz ? fz.i1 : fz.i0;
+                        if (iz < 0) continue;
+                        for (int cy = 0; cy < 2; ++cy) {
+                            const int iy = cy ? fy.i1 : fy.i0;
+                            if (iy < 0) continue;
+                            for (int cx = 0; cx < 2; ++cx) {
+                                const int ix = cx ? fx.i1 : fx.i0;
+                                if (ix < 0) continue;
+                                si[(size_t)k * 8 + t] = ix + nn * (iy + nn * iz);
+                                sw[(size_t)k * 8 + t] = (cx ? fx.w1 : fx.w0) * (cy ? fy.w1 : fy.w0) *
+                                                        (cz ? fz.w1 : fz.w0);
+                                ++t;
+                            }
+                        }
+                    }
+                    ++k;
+                }
+        // H_s = B_s^T H B_s
+        std::vector<cplx> hs((size_t)ds * ds);
+#pragma omp parallel for schedule(static)
+        for (int b = 0; b < ds; ++b)
+            for (int a = 0; a < ds; ++a) {
+                cplx acc = 0.0;
+                for (int u = 0; u < 8; ++u) {
+                    const int q = si[(size_t)b * 8 + u];
+                    if (q < 0) break;
+                    const cplx *col = h1 + (size_t)q * m;
+                    cplx part = 0.0;
+                    for (int t = 0; t < 8; ++t) {
+                        const int pidx = si[(size_t)a * 8 + t];
+                        if (pidx < 0) break;
+                        part += sw[(size_t)a * 8 + t] * col[pidx];
+                    }
+                    acc += sw[(size_t)b * 8 + u] * part;
+                }
+                hs[a + (size_t)ds * b] = acc;
+            }
+        std::vector<cplx> w;
+        DE_TRY(zgeev_right(ds, hs, w, vecs[sec]));
+        for (int c = 0; c < ds; ++c) levels.push_back({w[c], sec, c});
+    }
+    std::stable_sort(levels.begin(), levels.end(),
+                     [](const Level &x, const Level &y) { return x.w.real() < y.w.real(); });
+    energy.resize(numorbs);
+    orb.assign((size_t)m * numorbs, 0.0);
+    for (int k = 0; k < numorbs; ++k) {
+        const Level &L = levels[k];
+        energy[k] = L.w;
+        const int ds = dims[L.sector];
+        const cplx *y = vecs[L.sector].data() + (size_t)ds * L.col;
+        cplx *out = orb.data() + (size_t)m * k;
+        for (int a = 0; a < ds; ++a)
+            for (int t = 0; t < 8; ++t) {
+                const int pidx = sup_idx[L.sector][(size_t)a * 8 + t];
+                if (pidx < 0) break;
+                out[pidx] += sup_w[L.sector][(size_t)a * 8 + t] * y[a];
+            }
+    }
+    // HELIUM_ORBITALGATHER: modified Gram-Schmidt in level order
+    auto dotp = [&](const cplx *x, const cplx *y) {
+        cplx s = 0.0;
+        for (int64_t r = 0; r < m; ++r) s += (hermopt ? std::conj(x[r]) : x[r]) * y[r];
+        return s;
+    };
+    for (int i = 0; i < numorbs; ++i) {
+        cplx *xi = orb.data() + (size_t)i * m;
+        for (int j = 0; j < i; ++j) {
+            const cplx *xj = orb.data() + (size_t)j * m;
+            const cplx c = dotp(xj, xi);
+            for (int64_t r = 0; r < m; ++r) xi[r] -= xj[r] * c;
+        }
+        const cplx nrm = std::sqrt(dotp(xi, xi));
+        if (std::abs(nrm) == 0.0) return set_error(DE_E_INVALID, "orbital %d has zero norm after Gram-Schmidt", i);
+        for (int64_t r = 0; r < m; ++r) xi[r] /= nrm;
+    }
+    return DE_OK;
+}
+
+}  // namespace de
 
 extern "C" DE_API int de_subspace_guess_d(de_problem *h, int numorbs, int singlet, int hermopt, de_complex etarget,
                                          int numout, de_complex *x_d, de_complex *e0)
@@ -112,7 +254,7 @@ extern "C" DE_API int de_subspace_guess_d(de_problem *h, int numorbs, int single
     cudaStream_t st = h->stream;
     const int64_t m = h->m, d = h->dim;
 
-    // He+ orbitals: dense one-electron H, column j = H e_j
+    // He+ orbitals from the dense one-electron H, column j = H e_j
     if (numorbs > m)
         return set_error(DE_E_INVALID, "numorbs %d exceeds the %lld one-electron levels", numorbs, (long long)m);
     Handle1 h1;
@@ -134,30 +276,8 @@ extern "C" DE_API int de_subspace_guess_d(de_problem *h, int numorbs, int single
         DE_CUDA(cudaMemcpyAsync(a1.data(), h1d.p, a1.size() * sizeof(cplx), cudaMemcpyDeviceToHost, s1));
         DE_CUDA(cudaStreamSynchronize(s1));
     }
-    std::vector<cplx> w, vr;
-    DE_TRY(zgeev_right((int)m, a1, w, vr));
-    std::vector<int> idx(m);
-    std::iota(idx.begin(), idx.end(), 0);
-    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return w[x].real() < w[y].real(); });
-    // HELIUM_ORBITALGATHER hammod.F90:1084-1113: Gram-Schmidt of the orbitals
-    std::vector<cplx> orb((size_t)m * numorbs);
-    for (int a = 0; a < numorbs; ++a)
-        std::copy(vr.begin() + (size_t)idx[a] * m, vr.begin() + (size_t)(idx[a] + 1) * m, orb.begin() + (size_t)a * m);
-    auto dotp = [&](const cplx *x, const cplx *y) {
-        cplx s = 0.0;
-        for (int64_t r = 0; r < m; ++r) s += (hermopt ? std::conj(x[r]) : x[r]) * y[r];
-        return s;
-    };
-    for (int i = 0; i < numorbs; ++i) {
-        cplx *xi = orb.data() + (size_t)i * m;
-        for (int j = 0; j < i; ++j) {
-            const cplx *xj = orb.data() + (size_t)j * m;
-            const cplx c = dotp(xj, xi);
-            for (int64_t r = 0; r < m; ++r) xi[r] -= xj[r] * c;
-        }
-        const cplx nrm = std::sqrt(dotp(xi, xi));
-        for (int64_t r = 0; r < m; ++r) xi[r] /= nrm;
-    }
+    std::vector<cplx> energy, orb;
+    DE_TRY(heplus_orbitals(h->nn, a1.data(), numorbs, hermopt, energy, orb));
 
     // HELIUM_ORBITAL products (i <= j singlet, i < j triplet) and H times them
     std::vector<int2> pairs;
@@ -262,5 +382,17 @@ extern "C" DE_API int de_subspace_guess(de_problem *h, int numorbs, int singlet,
     DE_TRY(de_subspace_guess_d(h, numorbs, singlet, hermopt, etarget, numout, static_cast<de_complex *>(xd.p), e0));
     DE_CUDA(cudaMemcpyAsync(x, xd.p, bytes, cudaMemcpyDeviceToHost, xd.st));
     DE_CUDA(cudaStreamSynchronize(xd.st));
+    return DE_OK;
+}
+
+extern "C" DE_API int de_heplus_orbitals(int n, const de_complex *h1, int numorbs, int hermopt, de_complex *energies,
+                                        de_complex *orbitals)
+{
+    if (!h1 || !energies || !orbitals) return set_error(DE_E_INVALID, "null argument");
+    if (n < 0 || n > 11) return set_error(DE_E_INVALID, "N = %d is not in 0..11", n);
+    std::vector<cplx> energy, orb;
+    DE_TRY(heplus_orbitals(2 * n + 1, reinterpret_cast<const cplx *>(h1), numorbs, hermopt, energy, orb));
+    for (int k = 0; k < numorbs; ++k) energies[k] = de_complex{energy[k].real(), energy[k].imag()};
+    std::copy(orb.begin(), orb.end(), reinterpret_cast<cplx *>(orbitals));
     return DE_OK;
 }

@@ -230,6 +230,19 @@ DE_API int de_subspace_guess_d(de_problem *h, int numorbs, int singlet, int herm
 DE_API int de_subspace_guess(de_problem *h, int numorbs, int singlet, int hermopt, de_complex etarget,
                              int numout, de_complex *x, de_complex *e0);
 
+/* The He+ orbitals of the initial guess from a dense one-electron operator
+ * h1 (M x M, column-major, M = (2n+1)^3, n <= 11).  Host only: no GPU
+ * needed.  This replaces DIAGONALIZE (doublyexcited.F90:135-137) and
+ * HELIUM_ORBITALGATHER (hammod.F90:1084-1113).  The numorbs levels of
+ * lowest real part go to energies, and their right eigenvectors,
+ * Gram-Schmidt orthonormalised in that order, go to orbitals (M x numorbs,
+ * column-major).  The Gram-Schmidt uses c-products, or Hermitian products
+ * with hermopt.  The eigenproblem is split into the 8 reflection-parity
+ * sectors of the cube, one ZGEEV each.  de_subspace_guess uses this
+ * routine. */
+DE_API int de_heplus_orbitals(int n, const de_complex *h1, int numorbs, int hermopt, de_complex *energies,
+                              de_complex *orbitals);
+
 /* ---- eigensolver: GPLMR_EIG ----------------------------------------- */
 
 /* Block GPLMR with harmonic projection and the BASIC inner solve.
