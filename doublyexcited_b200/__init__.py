@@ -16,6 +16,8 @@ mirroring the reference's entry points (paths relative to
   (``DIAGSUBSPACE`` hammod.F90:1125-1256), and :func:`heplus_orbitals`, its
   He+ orbital step on the host
 * :func:`read_input`        -- ``get_input``/``get_args`` input.F90:143-362
+* :func:`run` / ``python -m doublyexcited_b200`` -- ``PROGRAM ATOM``
+  doublyexcited.F90:60-262
 * :func:`write_vectors` / :func:`read_vectors` -- utils.F90:82-198
 * :class:`Server` -- many independent solves on one GPU (no reference
   counterpart): admission by device footprint, concurrent streams
@@ -44,7 +46,7 @@ from ._lib import (  # noqa: F401
     lib,
     lib_path,
 )
-from .api import Problem, GplmrResult, Server, ServedResult, heplus_orbitals, read_input, read_vectors, vectors_header, write_vectors  # noqa: F401,E501
+from .api import Problem, GplmrResult, RunResult, Server, ServedResult, heplus_orbitals, read_input, read_vectors, run, vectors_header, write_vectors  # noqa: F401,E501
 
 __all__ = [
     "Problem",
@@ -52,6 +54,8 @@ __all__ = [
     "Server",
     "ServedResult",
     "heplus_orbitals",
+    "RunResult",
+    "run",
     "read_input",
     "read_vectors",
     "vectors_header",

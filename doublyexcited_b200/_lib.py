@@ -95,6 +95,17 @@ class de_input(ctypes.Structure):
     ]
 
 
+class de_run_info(ctypes.Structure):
+    _fields_ = [
+        ("totget", ctypes.c_int),
+        ("nexpects", ctypes.c_int),
+        ("e0", de_complex * 16),
+        ("expects", de_complex * 16),
+        ("shift", de_complex),
+        ("stats", de_stats),
+    ]
+
+
 class de_server_opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_int), ("max_bytes", ctypes.c_int64)]
 
@@ -166,6 +177,7 @@ SIGNATURES = {
     "de_subspace_guess": (INT, [P, INT, INT, INT, de_complex, INT, P, P]),
     "de_subspace_guess_d": (INT, [P, INT, INT, INT, de_complex, INT, P, P]),
     "de_heplus_orbitals": (INT, [INT, P, INT, INT, P, P]),
+    "de_run": (INT, [ctypes.POINTER(de_input), INT, P, P, ctypes.POINTER(de_run_info)]),
     "de_gplmr_eig": (INT, [P, P, P, I64, I64, de_complex, INT, INT, INT, ctypes.c_double,
                            ctypes.POINTER(de_gmres), INT, ctypes.POINTER(de_stats)]),
     "de_gplmr_eig_d": (INT, [P, P, P, I64, I64, de_complex, INT, INT, INT, ctypes.c_double,

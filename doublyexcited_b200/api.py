@@ -211,6 +211,56 @@ def heplus_orbitals(n: int, h1: np.ndarray, numorbs: int, hermopt: bool = False)
     return w, orb
 
 
+@dataclass
+class RunResult:
+    e: np.ndarray
+    x: np.ndarray
+    totget: int
+    e0: np.ndarray
+    expects: np.ndarray
+    shift: complex
+    iterations: int
+    converged: bool
+    max_residual: float
+
+
+def _parsed_input(path: str | None, argv: list[str] | None) -> de_input:
+    L = lib()
+    inp = de_input()
+    L.de_input_default(ctypes.byref(inp))
+    args = [a.encode() for a in (argv or [])]
+    arr = (ctypes.c_char_p * max(1, len(args)))(*args)
+    check(L.de_read_input(path.encode() if path else None, len(args), arr, ctypes.byref(inp)),
+          "de_read_input")
+    return inp
+
+
+def run(argv: list[str] | None = None, path: str | None = None, verbose: bool = False) -> RunResult:
+    """PROGRAM ATOM (doublyexcited.F90:60-262): the input file (path, else the
+    Inp= key of argv, else Input.Inp) and argv's keys, then the initial guess
+    or READVECS, NUMSKIP, the shift from GET_EXPECTS, GPLMR_EIG and WRITEVECS."""
+    argv = list(argv or [])
+    if path is None:
+        buf = ctypes.create_string_buffer(400)
+        args = [a.encode() for a in argv]
+        arr = (ctypes.c_char_p * max(1, len(args)))(*args)
+        check(lib().de_input_file_arg(len(args), arr, buf, len(buf)), "de_input_file_arg")
+        path = buf.value.decode()
+    inp = _parsed_input(path, argv)
+    nev = inp.gplmr_nev
+    dim = (2 * inp.params.n + 1) ** 6
+    x = np.empty((dim, max(nev, 1)), np.complex128, order="F")
+    e = np.empty(max(nev, 1), np.complex128)
+    info = _l.de_run_info()
+    check(lib().de_run(ctypes.byref(inp), int(bool(verbose)), _ptr(e), _ptr(x), ctypes.byref(info)), "de_run")
+    k = info.nexpects
+    e0 = np.array([complex(z.re, z.im) for z in info.e0[:k]])
+    ex = np.array([complex(z.re, z.im) for z in info.expects[:k]])
+    st = info.stats
+    return RunResult(e, x, info.totget, e0, ex, complex(info.shift.re, info.shift.im), st.iterations,
+                     bool(st.converged), st.max_residual)
+
+
 def read_input(path: str | None, argv: list[str] | None = None) -> dict:
     """Input.Inp namelists + command-line keys (get_input / get_args)."""
     L = lib()

@@ -304,6 +304,34 @@ DE_API int de_read_vectors(const char *path, int64_t m, int num, de_complex *psi
 /* Header of an eigenvector file: its M and number of vectors. */
 DE_API int de_vectors_header(const char *path, int64_t *m, int *num);
 
+/* ---- the whole program: PROGRAM ATOM ---------------------------------- */
+
+typedef struct {
+    int totget;              /* start vectors formed or read (TOTGET) */
+    int nexpects;            /* TOTGET - NUMSKIP */
+    de_complex e0[16];       /* subspace eigenvalues after NUMSKIP (zero when vectors were read) */
+    de_complex expects[16];  /* expectation values of the start vectors (GET_EXPECTS) */
+    de_complex shift;        /* the shift GPLMR ran with */
+    de_stats stats;
+} de_run_info;
+
+/* PROGRAM ATOM doublyexcited.F90:60-262 on a parsed input.  Steps:
+ *  1. TOTGET = min(MAXGET, NEV+NUMSKIP+5) start vectors from the initial
+ *     guess (de_subspace_guess, etarget = gplmr_shift), or NEV+NUMSKIP read
+ *     from invecfile when readvecs.  NEV+NUMSKIP above MAXGET returns
+ *     DE_E_INVALID (the reference STOPs: "GPLMR_NEV TOO BIG FOR NUMORBS").
+ *  2. NUMSKIP leading vectors are dropped.
+ *  3. GET_EXPECTS runs on the rest.  The shift is the mean of the first NEV
+ *     expectation values, real part only with takerealpart.
+ *  4. GPLMR_EIG runs with the input's NS, MAXIT, TOL and gmres options.
+ *  5. The NEV eigenvectors are written to outvecfile when writevecs.
+ * e receives NEV eigenvalues; x (may be NULL) the D x NEV eigenvectors;
+ * info (may be NULL) the intermediate values.  verbose prints the
+ * reference's report lines (SUBSPACE EIGENVALS, CHOSEN SHIFT, the GPLMR
+ * iterations every outmodulus, FINAL EIGVALS).  At most 16 start vectors.
+ * Argument errors return before any GPU work. */
+DE_API int de_run(const de_input *in, int verbose, de_complex *e, de_complex *x, de_run_info *info);
+
 /* ---- batched and served solves ----------------------------------------
  * No counterpart in the reference, which runs one GPLMR_EIG per MPI job
  * (doublyexcited.F90:238-241); these entry points run many independent

@@ -1,0 +1,31 @@
+"""de_run (PROGRAM ATOM, doublyexcited.F90:60-262) on the host: the checks
+the reference makes before any operator work, here made before any GPU
+work, and the loud failure without a GPU."""
+import pytest
+
+
+def test_run_rejects_nev_above_the_guess_products(de, tmp_path):
+    """Two orbitals give one triplet product; NEV=2 is the reference's
+    "GPLRM_NEV TOO BIG FOR NUMORBS" stop (doublyexcited.F90:143-148)."""
+    with pytest.raises(de.DeError) as e:
+        de.run(["N=2", "Nev=2", "Norbs=2", "Trip"], path=str(tmp_path / "absent.inp"))
+    assert e.value.status == de.DE_E_INVALID
+    assert "TOO BIG" in str(e.value)
+
+
+def test_run_rejects_more_than_16_start_vectors(de, tmp_path):
+    """TOTGET = min(MAXGET, NEV+NUMSKIP+5) = 18 start vectors."""
+    with pytest.raises(de.DeError) as e:
+        de.run(["N=2", "Nev=8", "Skip=5", "Norbs=10", "Sing"], path=str(tmp_path / "absent.inp"))
+    assert e.value.status == de.DE_E_INVALID
+    assert "TOTGET" in str(e.value)
+
+
+def test_run_fails_loudly_without_gpu(de, tmp_path):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(de.DeError) as e:
+        de.run(["N=2", "Nev=1", "Norbs=3", "Sing"], path=str(tmp_path / "absent.inp"))
+    assert e.value.status == de.DE_E_CUDA

@@ -1,0 +1,35 @@
+"""de_run (PROGRAM ATOM, doublyexcited.F90:60-262) on the GPU: an Input.Inp
+run equals the same steps made one by one through the C ABI.  The steps
+are the initial guess, GET_EXPECTS, the shift as the real part of the mean
+expectation value, GPLMR_EIG, and WRITEVECS.  Bars: guess and expectation
+values to 1e-12, the eigenvalue after a fixed 8 iterations to 1e-10, the
+written file equal to the returned vectors.  (The file name sorts last: the
+suite stops at its first failure and this test is the newest.)"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_run_replays_the_program_step_by_step(de, tmp_path):
+    inp = tmp_path / "Input.Inp"
+    out = tmp_path / "eigvecs.out"
+    inp.write_text("&main\n WRITEVECS=.TRUE.\n/\n"
+                   "&grid\n AUTODELTA=.false.\n DELTA=2d0\n N=3\n/\n"
+                   "&orbitals\n NUMORBS=5\n SINGLET=T\n/\n"
+                   "&gplmr\n GPLMR_SHIFT=(-0.78d0,0d0)\n GPLMR_MAXIT=8\n GPLMR_TOL=1D-14\n GPLMR_NEV=1\n/\n")
+    # a list-directed read ends an unquoted value at '/': paths are quoted
+    r = de.run([f"Inp={inp}", "Theta=0.3", f"Outfile='{out}'"])
+    assert r.totget == 6  # min(MAXGET = 15, NEV + NUMSKIP + 5)
+    with de.Problem(n=3, delta=2.0, theta=0.3) as h:
+        e0, x0 = h.subspace_guess(5, True, False, -0.78, 6)
+        ex = h.get_expects(x0)
+        sigma = complex(ex[0].real, 0.0)
+        g = h.gplmr_eig(x0[:, :1], sigma, ns=5, maxit=8, tol=1e-14, max_inner_iter=5)
+    assert np.max(np.abs(r.e0 - e0)) < 1e-12
+    assert np.max(np.abs(r.expects - ex)) < 1e-12
+    assert abs(r.shift - sigma) < 1e-12
+    assert r.iterations == g.iterations == 8
+    assert abs(r.e[0] - g.e[0]) < 1e-10
+    back = de.read_vectors(str(out), 7 ** 3, 1)
+    assert np.array_equal(back[:, 0], r.x[:, 0])
