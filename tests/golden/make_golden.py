@@ -129,6 +129,8 @@ FIXTURES = {
     "hammult_n2": (False, lambda: ("npz", hammult_fixture(2, 0.3, 12, True))),
     "hammult_n3": (False, lambda: ("npz", hammult_fixture(3, 0.35, 13, False))),
     "hammult_n4": (False, lambda: ("npz", hammult_fixture(4, 0.2, 14, False))),
+    "hammult_n5": (False, lambda: ("npz", hammult_fixture(5, 0.35, 15, False))),
+    "hammult_n6": (False, lambda: ("npz", hammult_fixture(6, 0.2, 16, False))),
     "hammult1_n5": (False, lambda: ("npz", hammult1_fixture(5, 0.2, 15))),
     "gplmr_n3_nev1": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 1, False, 60, 1e-10))),
     "gplmr_n3_nev4": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 4, False, 12, 1e-10))),

@@ -56,7 +56,7 @@ def test_hammult_full_golden(de, name):
         assert rel_err(g.hammult(a["x"]), a["y"]) < TOL
 
 
-@pytest.mark.parametrize("name", ["hammult_n3.npz", "hammult_n4.npz"])
+@pytest.mark.parametrize("name", ["hammult_n3.npz", "hammult_n4.npz", "hammult_n5.npz", "hammult_n6.npz"])
 def test_hammult_sampled_golden(de, oracle, name):
     meta, a = load_npz(name)
     p = oracle.Params(n=meta["n"], delta=meta["delta"], theta=meta["theta"])

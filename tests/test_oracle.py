@@ -78,7 +78,7 @@ def test_oracle_reproduces_full_golden(oracle, name):
     assert rel_err(h.matvec(a["x"]), a["y"]) < 1e-14
 
 
-@pytest.mark.parametrize("name", ["hammult_n3.npz", "hammult_n4.npz"])
+@pytest.mark.parametrize("name", ["hammult_n3.npz", "hammult_n4.npz", "hammult_n5.npz", "hammult_n6.npz"])
 def test_oracle_reproduces_sampled_golden(oracle, name):
     meta, a = load_npz(name)
     p = oracle.Params(n=meta["n"], delta=meta["delta"], theta=meta["theta"])
