@@ -64,6 +64,10 @@ struct Solver {
     double2 *X = nullptr, *AX = nullptr, *W = nullptr, *AW = nullptr;
     double2 *S = nullptr, *AS = nullptr, *P = nullptr, *AP = nullptr;
     double2 *LV = nullptr, *LQ = nullptr;  // inner solve: order*nev each
+    // PETSc-style GMRES inner solve (usepetscflag = 0): basis columns, the
+    // iterate and the residual; small device scalars
+    static constexpr int kGmresRestart = 30;
+    double2 *GV = nullptr, *dGs = nullptr;
     float2 *LV32 = nullptr, *LQ32 = nullptr;  // the same in complex64 (mixed)
     bool mixed = false;
     double exch_sign = 0.0;  // +1 / -1: exchange symmetry of the start block (mixed form), 0: none
@@ -105,7 +109,10 @@ struct Solver {
             DE_TRY(alloc(&S, D * ldr));
             DE_TRY(alloc(&AS, D * ldr));
         }
-        if (order > 0) {
+        if (order > 1 && gm.usepetscflag == 0) {  // GMRES: basis, iterate, residual
+            DE_TRY(alloc(&GV, D * (int64_t)(std::min(order, kGmresRestart) + 3)));
+            DE_TRY(alloc(&dGs, 128));
+        } else if (order > 0) {
             const int64_t n = D * (int64_t)std::max(1, order) * nev;
             if (mixed && order > 1) {  // complex64: half the bytes
                 DE_TRY(alloc(reinterpret_cast<double2 **>(&LV32), (n + 1) / 2));
@@ -645,6 +652,128 @@ struct Solver {
         return updateT(V, thisdim, b, k, dC, thisdim);
     }
 
+    // |v|^2 into dout[0] on the device and into *host
+    int sqnorm(const double2 *v, double2 *dout, double *host)
+    {
+        const double2 *a[1] = {v};
+        cudaError_t e = dotdiag_launch(a, a, 1, D, 1, dout, h->d_work, st);
+        if (e != cudaSuccess) return cuda_error(e, "dotdiag");
+        DE_CUDA(cudaMemcpyAsync(hbuf, dout, sizeof(double2), cudaMemcpyDeviceToHost, st));
+        DE_CUDA(cudaStreamSynchronize(st));
+        *host = hbuf[0].x;
+        return DE_OK;
+    }
+
+    // v *= 1/sqrt(|n2[0]|), n2 a device scalar (n2[1] receives the factor)
+    int scale_by_inv_norm(double2 *v, double2 *n2)
+    {
+        cudaError_t e = inv_sqrt_abs_launch(n2, n2 + 1, 1, st);
+        if (e != cudaSuccess) return cuda_error(e, "inv_sqrt");
+        double2 *w[1] = {v};
+        if ((e = scale_cols_launch(w, 1, n2 + 1, D, st)) != cudaSuccess) return cuda_error(e, "scale");
+        return DE_OK;
+    }
+
+    // PRECBLOCK_PETSC gplmr.F90:507-563: b_j <- GMRES solution of
+    // (H - shift) x = b_j, column by column, in the configuration PETSCSOLVE
+    // petscsolve.F90:142-279 gives KSPGMRES.  PETSc's defaults apply: restart
+    // 30, classical Gram-Schmidt without refinement (one Gram of the basis
+    // against w, then one update), no preconditioner (GM_PCOPT = 0 on a shell
+    // operator), zero initial guess.  KSPSetTolerances sets rtol = GM_TOL and
+    // max_it = GM_MAX_INNER_ITER; the default test stops when the Arnoldi
+    // residual estimate |g_{k+1}| <= max(rtol ||b||, 1e-50), or at a happy
+    // breakdown.  The shift is the reference's GMSOLVER%SHIFT, which nothing
+    // assigns: its main-program storage is zero, so the operator is H.
+    int gmres_col(double2 *b)
+    {
+        const int max_it = gm.max_inner_iter;
+        const int mk = std::min(max_it, kGmresRestart);
+        double2 *V = GV, *xg = GV + (int64_t)(mk + 1) * D, *r = xg + D;
+        double2 *dn2 = dGs + 64, *dy = dGs + 80;
+        double bn2 = 0.0;
+        DE_TRY(sqnorm(b, dn2, &bn2));
+        const double bnorm = std::sqrt(bn2), ttol = std::max(gm.tol * bnorm, 1e-50);
+        if (bnorm <= ttol) {  // converged at iteration 0: x = 0
+            DE_CUDA(cudaMemsetAsync(b, 0, D * sizeof(double2), st));
+            return DE_OK;
+        }
+        DE_CUDA(cudaMemcpyAsync(r, b, D * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+        int its = 0;
+        bool first = true, done = false;
+        double beta2 = bn2;
+        std::vector<cplx> hh((size_t)(mk + 1) * mk), g(mk + 1), cs(mk), sn(mk), c(mk + 1);
+        while (!done) {
+            if (!first) DE_TRY(sqnorm(r, dn2, &beta2));
+            DE_CUDA(cudaMemcpyAsync(V, r, D * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+            DE_TRY(scale_by_inv_norm(V, dn2));
+            std::fill(g.begin(), g.end(), cplx(0.0));
+            g[0] = std::sqrt(beta2);
+            int k = 0;
+            while (k < mk && its < max_it) {
+                double2 *w = col(V, k + 1);
+                DE_TRY(matblock(col(V, k), w, 1));
+                DE_TRY(gram_dev(cols(V, k + 1, D), cols(w, 1, D), dGs, k + 1));
+                DE_TRY(update(cl(V, k + 1), {w}, dGs, k + 1, -1.0, 1.0));
+                const double2 *a[1] = {w};
+                cudaError_t e = dotdiag_launch(a, a, 1, D, 1, dn2, h->d_work, st);
+                if (e != cudaSuccess) return cuda_error(e, "dotdiag");
+                DE_CUDA(cudaMemcpyAsync(hbuf, dGs, 65 * sizeof(double2), cudaMemcpyDeviceToHost, st));
+                DE_CUDA(cudaStreamSynchronize(st));
+                const double tt = std::sqrt(hbuf[64].x);
+                for (int i = 0; i <= k; ++i) c[i] = cplx(hbuf[i].x, hbuf[i].y);
+                c[k + 1] = tt;
+                for (int i = 0; i < k; ++i) {  // earlier rotations
+                    const cplx a0 = c[i], a1 = c[i + 1];
+                    c[i] = std::conj(cs[i]) * a0 + sn[i] * a1;
+                    c[i + 1] = -std::conj(sn[i]) * a0 + cs[i] * a1;
+                }
+                const double hapbnd = std::min(g[k] != 0.0 ? std::abs(tt / g[k]) : 1e-30, 1e-30);
+                const bool hap = tt < hapbnd;
+                const double den = std::sqrt(std::norm(c[k]) + std::norm(c[k + 1]));
+                ++its;
+                if (den == 0.0) {  // KSP_DIVERGED_NULL: keep the earlier columns
+                    done = true;
+                    break;
+                }
+                cs[k] = c[k] / den;
+                sn[k] = c[k + 1] / den;
+                c[k] = den;
+                c[k + 1] = 0.0;
+                g[k + 1] = -std::conj(sn[k]) * g[k];
+                g[k] = std::conj(cs[k]) * g[k];
+                for (int i = 0; i <= k + 1; ++i) hh[i + (size_t)(mk + 1) * k] = c[i];
+                const double res = std::abs(g[k + 1]);
+                ++k;
+                if (res <= ttol || hap || its >= max_it) {
+                    done = true;
+                    break;
+                }
+                DE_TRY(scale_by_inv_norm(w, dn2));
+            }
+            // back substitution R y = g, then x (+)= V y
+            std::vector<cplx> y(k);
+            for (int i = k - 1; i >= 0; --i) {
+                cplx t = g[i];
+                for (int j = i + 1; j < k; ++j) t -= hh[i + (size_t)(mk + 1) * j] * y[j];
+                y[i] = t / hh[i + (size_t)(mk + 1) * i];
+            }
+            if (k > 0) {
+                DE_TRY(upload(y, dy));
+                DE_TRY(update(cl(V, k), {xg}, dy, k, 1.0, first ? 0.0 : 1.0));
+            } else if (first) {
+                DE_CUDA(cudaMemsetAsync(xg, 0, D * sizeof(double2), st));
+            }
+            first = false;
+            if (!done) {  // restart: r = b - (H - shift) x
+                DE_TRY(matblock(xg, r, 1));
+                cudaError_t e = axpy_launch(r, b, r, make_double2(-1.0, 0.0), D, st);
+                if (e != cudaSuccess) return cuda_error(e, "axpy");
+            }
+        }
+        DE_CUDA(cudaMemcpyAsync(b, xg, D * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+        return DE_OK;
+    }
+
     // PRECBLOCK gplmr.F90:466-502 (in place)
     int precblock(double2 *b, int k)
     {
@@ -657,7 +786,8 @@ struct Solver {
                 if (e != cudaSuccess) s = cuda_error(e, "copy");
             }
         } else if (gm.usepetscflag == 0) {
-            s = set_error(DE_E_UNSUPPORTED, "usepetscflag=0 selects the PETSc KSP inner solve, which this build does not provide");
+            s = DE_OK;
+            for (int j = 0; s == DE_OK && j < k; ++j) s = gmres_col(col(b, j));
         } else if (mixed) {
             s = basic<float2>(b, k);
             // FP32 rounding in the inner solve breaks the electron-exchange

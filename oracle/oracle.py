@@ -21,6 +21,9 @@ It restates, loop for loop where it matters, the Fortran reference
 * the inner solve ``basicblocklansolve``/``harm_orthog_oneblock``/
   ``fast_harmritz_setup``/``myhgramschmidt_many``
   harmonic_ritz_small.F90:28-324 and ``gen_cmatsub`` hr_eigen.f90:223-291;
+  the alternative ``PRECBLOCK_PETSC`` gplmr.F90:507-563 as GMRES in the
+  configuration ``PETSCSOLVE`` petscsolve.F90:142-279 sets (PETSc is absent:
+  the published algorithm, parity with PETSc itself unpinned);
 * ``GET_EXPECTS`` hammod.F90:1261-1301 and the shift rule
   doublyexcited.F90:214-219;
 * the initial guess: He+ orbitals (dense, where the reference runs block
@@ -401,10 +404,105 @@ def solve_gevp(kp: np.ndarray, mp: np.ndarray, k: int, nev: int) -> np.ndarray:
     return vr[:, idx]
 
 
+@dataclass
+class GmresResult:
+    x: np.ndarray
+    its: int
+    rnorm: float
+    reason: str
+
+
+def petsc_gmres(apply, b: np.ndarray, max_it: int, rtol: float, abstol: float = 1e-50,
+                restart: int = 30, haptol: float = 1e-30) -> GmresResult:
+    """KSPSolve as PETSCSOLVE petscsolve.F90:142-279 configures it, called
+    column by column from PRECBLOCK_PETSC gplmr.F90:507-563.  The settings:
+    KSPGMRES with PETSc's defaults, restart 30, classical Gram-Schmidt
+    without refinement, no preconditioner (GM_PCOPT = 0 and a shell
+    operator), zero initial guess.  KSPSetTolerances(rtol = GM_TOL,
+    max_it = GM_MAX_INNER_ITER).  The default test stops when the Arnoldi
+    residual estimate |g_{k+1}| <= max(rtol ||b||, abstol).  Inner products
+    are Hermitian.
+
+    PETSc is a third-party library absent here: this restates the published
+    GMRES algorithm in the structure of PETSc's KSPGMRESCycle (one operator
+    application per iteration, Givens rotations on the Hessenberg column,
+    back substitution at the end of a cycle; a restart recomputes
+    r = b - A x without counting an iteration)."""
+    b = np.asarray(b, dtype=np.complex128)
+    x = np.zeros_like(b)
+    bnorm = float(np.linalg.norm(b))
+    ttol = max(rtol * bnorm, abstol)
+    if bnorm <= ttol:
+        return GmresResult(x, 0, bnorm, "converged_atol")
+    its = 0
+    r = b.copy()
+    reason = ""
+    res = bnorm
+    while not reason:
+        beta = float(np.linalg.norm(r))
+        vs = [r / beta]
+        hh = np.zeros((restart + 1, restart), np.complex128)
+        g = np.zeros(restart + 1, np.complex128)
+        g[0] = beta
+        cs = np.zeros(restart, np.complex128)
+        sn = np.zeros(restart, np.complex128)
+        k = 0
+        while k < restart and its < max_it:
+            w = apply(vs[k])
+            coef = np.array([np.vdot(vs[i], w) for i in range(k + 1)])  # classical: all on w
+            for i in range(k + 1):
+                w = w - vs[i] * coef[i]
+            tt = float(np.linalg.norm(w))
+            col = np.zeros(restart + 1, np.complex128)
+            col[:k + 1] = coef
+            col[k + 1] = tt
+            for i in range(k):  # earlier rotations
+                a0, a1 = col[i], col[i + 1]
+                col[i] = np.conj(cs[i]) * a0 + sn[i] * a1
+                col[i + 1] = -np.conj(sn[i]) * a0 + cs[i] * a1
+            hap = tt < min(abs(tt / g[k]) if g[k] != 0 else haptol, haptol)
+            den = math.sqrt(abs(col[k]) ** 2 + abs(col[k + 1]) ** 2)
+            if den == 0.0:  # KSP_DIVERGED_NULL: keep the earlier columns
+                its += 1
+                reason = "diverged_null"
+                break
+            cs[k], sn[k] = col[k] / den, col[k + 1] / den
+            col[k] = den
+            col[k + 1] = 0.0
+            g[k + 1] = -np.conj(sn[k]) * g[k]
+            g[k] = np.conj(cs[k]) * g[k]
+            hh[:, k] = col
+            res = abs(g[k + 1])
+            k += 1
+            its += 1
+            if res <= ttol:
+                reason = "converged_rtol"
+            elif hap:
+                reason = "happy_breakdown"
+            elif its >= max_it:
+                reason = "diverged_its"
+            if reason:
+                break
+            vs.append(w / tt)
+        y = np.zeros(k, np.complex128)
+        for i in range(k - 1, -1, -1):
+            y[i] = (g[i] - hh[i, i + 1:k] @ y[i + 1:k]) / hh[i, i]
+        for i in range(k):
+            x = x + vs[i] * y[i]
+        if not reason:
+            r = b - apply(x)
+    return GmresResult(x, its, res, reason)
+
+
 def gplmr_eig(h: Hamiltonian, x0: np.ndarray, sigma: complex, ns: int = 5, maxit: int = 100,
               tol: float = 1e-7, order: int = 5, compat_first_column_only: bool = False,
-              max_inner_iter: int | None = None, verbose: bool = False) -> GplmrResult:
-    """GPLMR_EIG gplmr.F90:9-374 with the BASIC preconditioner."""
+              max_inner_iter: int | None = None, verbose: bool = False, usepetscflag: int = 1,
+              gm_tol: float = 1e-3, gm_shift: complex = 0.0) -> GplmrResult:
+    """GPLMR_EIG gplmr.F90:9-374 with the BASIC preconditioner, or with
+    usepetscflag = 0 the PETSc GMRES one (PRECBLOCK gplmr.F90:466-502):
+    GMRES on (H - gm_shift) per column with rtol gm_tol.  The reference's
+    GMSOLVER%SHIFT is never assigned and lives in the main program's
+    zero-initialised storage, so gm_shift defaults to 0."""
     if max_inner_iter is None:
         max_inner_iter = order
     calls0 = h.calls
@@ -416,6 +514,12 @@ def gplmr_eig(h: Hamiltonian, x0: np.ndarray, sigma: complex, ns: int = 5, maxit
     def precblock(blk: np.ndarray) -> np.ndarray:
         if max_inner_iter == 1:
             return h.matblock(blk)
+        if usepetscflag == 0:
+            out = np.empty_like(blk)
+            for j in range(blk.shape[1]):
+                out[:, j] = petsc_gmres(lambda v: h.matvec(v) - gm_shift * v, blk[:, j], max_inner_iter,
+                                        gm_tol).x
+            return out
 
         def mult(v: np.ndarray) -> np.ndarray:
             if compat_first_column_only:

@@ -90,7 +90,7 @@ def hammult1_fixture(n, theta, seed):
     return {"n": n, "delta": 2.0, "theta": theta, "seed": seed}, {"x": x, "y": y}
 
 
-def gplmr_fixture(n, theta, sigma, nev, compat, maxit, tol, seed=0, spin="singlet"):
+def gplmr_fixture(n, theta, sigma, nev, compat, maxit, tol, seed=0, spin="singlet", usepetscflag=1):
     p = O.Params(n=n, delta=2.0, theta=theta)
     h = O.init_hamiltonian(p, nelec=2)
     x0 = O.seeded_start(p, nev, seed, spin)
@@ -99,10 +99,11 @@ def gplmr_fixture(n, theta, sigma, nev, compat, maxit, tol, seed=0, spin="single
         "params": {"n": n, "delta": 2.0, "theta": theta, "charge": 2.0},
         "start": {"kind": "seeded_start", "seed": seed, "spin": spin, "nev": nev},
         "solver": {"sigma": _c(sigma), "ns": 5, "order": 5, "maxit": maxit, "tol": tol,
-                   "compat_first_column_only": bool(compat)},
+                   "compat_first_column_only": bool(compat), "usepetscflag": usepetscflag, "gm_tol": 1e-3},
     }
     try:
-        r = O.gplmr_eig(h, x0, sigma, ns=5, maxit=maxit, tol=tol, order=5, compat_first_column_only=compat)
+        r = O.gplmr_eig(h, x0, sigma, ns=5, maxit=maxit, tol=tol, order=5, compat_first_column_only=compat,
+                        usepetscflag=usepetscflag, gm_tol=1e-3)
     except O.OrthoCheckFailed as e:
         # With NEV > 1 the first-column-only product of the reference's
         # allhmultsub is not linear in the block, so harm_orthog_oneblock's
@@ -113,7 +114,7 @@ def gplmr_fixture(n, theta, sigma, nev, compat, maxit, tol, seed=0, spin="single
         "params": {"n": n, "delta": 2.0, "theta": theta, "charge": 2.0},
         "start": {"kind": "seeded_start", "seed": seed, "spin": spin, "nev": nev},
         "solver": {"sigma": _c(sigma), "ns": 5, "order": 5, "maxit": maxit, "tol": tol,
-                   "compat_first_column_only": bool(compat)},
+                   "compat_first_column_only": bool(compat), "usepetscflag": usepetscflag, "gm_tol": 1e-3},
         "iterations": r.iterations,
         "matvecs_reference": r.matvecs,
         "e": [_c(z) for z in r.e],
@@ -135,6 +136,10 @@ FIXTURES = {
     "gplmr_n3_nev1": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 1, False, 60, 1e-10))),
     "gplmr_n3_nev4": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 4, False, 12, 1e-10))),
     "gplmr_n3_nev4_compat": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 4, True, 12, 1e-10))),
+    "gplmr_n3_nev1_petsc": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 1, False, 80, 1e-10,
+                                                                 usepetscflag=0))),
+    "gplmr_n3_nev2_petsc": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 2, False, 6, 1e-10,
+                                                                 usepetscflag=0))),
     "gplmr_n5_nev1": (True, lambda: ("json", gplmr_fixture(5, 0.2, complex(-0.7131541429, 0), 1, False, 60, 1e-9))),
     "gplmr_n6_nev1": (True, lambda: ("json", gplmr_fixture(6, 0.2, complex(-0.7131541429, 0), 1, False, 80, 1e-8))),
 }

@@ -126,15 +126,6 @@ def test_gplmr_iteration_history_prefix(de, oracle):
     assert abs(r.e[0] - e) < 1e-10
 
 
-def test_petsc_path_is_unsupported(de, oracle):
-    p = oracle.Params(n=2, delta=2.0, theta=0.3)
-    x0 = oracle.seeded_start(p, 1, 0)
-    with de.Problem(n=2, delta=2.0, theta=0.3) as h:
-        with pytest.raises(de.DeError) as e:
-            h.gplmr_eig(x0, -0.78, maxit=2, usepetscflag=0)
-        assert e.value.status == de.DE_E_UNSUPPORTED
-
-
 def test_matvec_accounting(de, oracle):
     """ICALLED accounting of the reference: per iteration (1+NS)*NEV MATBLOCK
     products plus (1+NS) PRECBLOCK calls of (2*order+1) products each (NEV

@@ -138,3 +138,59 @@ def test_subspace_guess_matches_reference_log(oracle):
         assert np.max(np.abs(xm - xm.T)) < 1e-12
     hx = h2.matvec(x[:, 0])
     assert abs(np.dot(x[:, 0], hx) / np.dot(x[:, 0], x[:, 0]) - e0[0]) < 1e-10
+
+
+def _krylov_minimizer(a, b, k):
+    """argmin ||b - A x|| over span{b, Ab, ..., A^(k-1) b}, by an orthonormal
+    basis and a dense least-squares solve (the definition GMRES computes)."""
+    kb = np.empty((b.size, k), np.complex128)
+    kb[:, 0] = b
+    for j in range(1, k):
+        kb[:, j] = a @ kb[:, j - 1]
+    q, _ = np.linalg.qr(kb)
+    c, *_ = np.linalg.lstsq(a @ q, b, rcond=None)
+    return q @ c
+
+
+def test_petsc_gmres_is_the_krylov_minimizer(oracle):
+    """The GMRES restatement behind PRECBLOCK_PETSC: after k iterations from
+    a zero guess, x_k minimises the residual over the k-th Krylov space, and
+    its residual estimate equals the true residual."""
+    rng = np.random.default_rng(7)
+    n = 80
+    a = np.diag(np.linspace(1.0, 3.0, n) + 0.3j) + 0.1 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    for k in (1, 2, 5, 8):
+        r = oracle.petsc_gmres(lambda v: a @ v, b, max_it=k, rtol=1e-300)
+        assert r.its == k and r.reason == "diverged_its"
+        xk = _krylov_minimizer(a, b, k)
+        assert np.linalg.norm(r.x - xk) < 1e-10 * np.linalg.norm(xk)
+        assert abs(r.rnorm - np.linalg.norm(b - a @ r.x)) < 1e-10 * np.linalg.norm(b)
+
+
+def test_petsc_gmres_stops_at_rtol_and_restarts(oracle):
+    rng = np.random.default_rng(8)
+    n = 60
+    a = np.diag(np.linspace(1.0, 2.0, n) + 0.2j) + 0.05 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    bn = np.linalg.norm(b)
+    res = [np.linalg.norm(b - a @ _krylov_minimizer(a, b, k)) for k in range(1, 12)]
+    rtol = 0.5 * (res[3] + res[4]) / bn  # crossed at the 5th iteration
+    r = oracle.petsc_gmres(lambda v: a @ v, b, max_it=30, rtol=rtol)
+    assert r.reason == "converged_rtol" and r.its == 5
+    # GMRES(3): each cycle minimises over the Krylov space of its own residual
+    r = oracle.petsc_gmres(lambda v: a @ v, b, max_it=7, rtol=1e-300, restart=3)
+    x = np.zeros(n, np.complex128)
+    for k in (3, 3, 1):
+        x = x + _krylov_minimizer(a, b - a @ x, k)
+    assert r.its == 7 and np.linalg.norm(r.x - x) < 1e-10 * np.linalg.norm(x)
+
+
+def test_gmres_and_basic_inner_solves_find_the_same_resonance():
+    """The oracle's GPLMR with the PETSc-style GMRES inner solve
+    (usepetscflag = 0) and with the BASIC one converge, from the same start,
+    to the same N=3 resonance: the inner solve only preconditions."""
+    a = load_json("gplmr_n3_nev1_petsc.json")
+    b = load_json("gplmr_n3_nev1.json")
+    assert a["solver"]["usepetscflag"] == 0
+    assert abs(complex(*a["e"][0]) - complex(*b["e"][0])) < 1e-10
