@@ -48,7 +48,7 @@ enum {
     DE_E_SIZE = 2,         /* size mismatch (reference: "SIZE ERRORRRR 66", doublyexcited.F90:33-36) */
     DE_E_CUDA = 3,         /* CUDA runtime error */
     DE_E_NOMEM = 4,        /* device or host allocation failed */
-    DE_E_UNSUPPORTED = 5,  /* option the build does not provide (e.g. PETSc inner solve) */
+    DE_E_UNSUPPORTED = 5,  /* option the build does not provide (e.g. grids above N=11) */
     DE_E_CHOLESKY = 6,     /* zpotrf breakdown in cholQR (lamod.f90:169-175) */
     DE_E_GEVP = 7,         /* zggev failure (gplmr.F90:431-432) */
     DE_E_SVD = 8,          /* zgesdd failure (hr_eigen.f90:246-248) */
@@ -82,10 +82,13 @@ typedef struct {
 
 /* Inner-solve options.  Mirrors GMRES_SOLVER (structs.F90:137-162). */
 typedef struct {
-    int max_inner_iter;          /* GM_MAX_INNER_ITER: Krylov order of PRECBLOCK_BASIC */
-    int usepetscflag;            /* 0 -> PETSc KSP path (not built: DE_E_UNSUPPORTED); else BASIC.
+    int max_inner_iter;          /* GM_MAX_INNER_ITER: Krylov order of PRECBLOCK_BASIC, or the
+                                    GMRES iteration limit of the PETSc path */
+    int usepetscflag;            /* 0 -> the PETSc path: per column, GMRES on H in KSPGMRES's
+                                    configuration (PRECBLOCK_PETSC gplmr.F90:507-563,
+                                    PETSCSOLVE petscsolve.F90:142-279), FP64; else BASIC.
                                     The reference's flag is inverted (gplmr.F90:496-500); same here. */
-    double tol;                  /* GM_TOL (used by the PETSc path only) */
+    double tol;                  /* GM_TOL: the GMRES rtol (PETSc path only) */
     int compat_first_column_only;/* 1: reproduce allhmultsub's first-column-only matvec
                                     (gplmr.F90:704-716); other columns of the product are zero */
 } de_gmres;
