@@ -263,13 +263,7 @@ def run(argv: list[str] | None = None, path: str | None = None, verbose: bool = 
 
 def read_input(path: str | None, argv: list[str] | None = None) -> dict:
     """Input.Inp namelists + command-line keys (get_input / get_args)."""
-    L = lib()
-    inp = de_input()
-    L.de_input_default(ctypes.byref(inp))
-    args = [a.encode() for a in (argv or [])]
-    arr = (ctypes.c_char_p * max(1, len(args)))(*args)
-    check(L.de_read_input(path.encode() if path else None, len(args), arr, ctypes.byref(inp)),
-          "de_read_input")
+    inp = _parsed_input(path, argv)
     p = inp.params
     return {
         "N": p.n, "DELTA": p.delta, "RADIUS": p.radius, "AUTODELTA": bool(p.autodelta), "THETA": p.theta,
