@@ -29,3 +29,18 @@ def test_run_fails_loudly_without_gpu(de, tmp_path):
     with pytest.raises(de.DeError) as e:
         de.run(["N=2", "Nev=1", "Norbs=3", "Sing"], path=str(tmp_path / "absent.inp"))
     assert e.value.status == de.DE_E_CUDA
+
+
+def test_command_line_reports_input_errors(tmp_path):
+    """python -m doublyexcited_b200 prints the reference's message and exits
+    with the DE_E_* status, without a traceback."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    p = subprocess.run([sys.executable, "-m", "doublyexcited_b200", "N=2", "Nev=2", "Norbs=2", "Trip"],
+                       cwd=tmp_path, capture_output=True, text=True, timeout=300,
+                       env={**os.environ, "PYTHONPATH": root})
+    assert p.returncode == 1  # DE_E_INVALID
+    assert "TOO BIG FOR NUMORBS" in p.stderr and "Traceback" not in p.stderr
