@@ -510,6 +510,9 @@ def main():
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip the plain-FP64 solves timed beside the mixed ones")
     ap.add_argument("--workers", type=int, default=None, help="serve: concurrent solves (CUDA streams)")
+    ap.add_argument("--start", default="seeded", choices=["seeded", "guess"],
+                    help="solve workloads: seeded complex-Gaussian start block, or the reference's initial "
+                         "guess (de_subspace_guess: 14 He+ orbitals, etarget = sigma), formed before timing")
     ap.add_argument("--maxit", type=int, default=None,
                     help="cap the GPLMR iterations (short runs for kernel profiling; not a bench value)")
     a = ap.parse_args()
@@ -558,7 +561,10 @@ def main():
         """W untimed + K timed solves at one precision, device-timed."""
         prob = de.Problem(n=w["n"], delta=w["delta"], theta=w["theta"], device=local, precision=precision)
         prob.set_stream(stream.cuda_stream)
-        x0 = seeded_start(prob.m, w["nev"], w["seed"], w["spin"])
+        if a.start == "guess":
+            _, x0 = prob.subspace_guess(14, w["spin"] == "singlet", False, w["sigma"], w["nev"])
+        else:
+            x0 = seeded_start(prob.m, w["nev"], w["seed"], w["spin"])
         dim = prob.dim
         x0_dev = torch.from_numpy(np.ascontiguousarray(x0.T)).to("cuda")  # (nev, dim): columns contiguous
         x_dev = torch.empty_like(x0_dev)
@@ -703,8 +709,11 @@ def main():
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": elapsed / a.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if a.precision == "fp64" else "f32 inner solve / f64 outer iteration",
-            "data": "synthetic (seeded complex-Gaussian singlet start vector; operator from the reference's physics)",
-            "config": {"workload": a.workload, "N": w["n"], "NN": nn, "dim": dim, "nev": w["nev"], "ns": w["ns"],
+            "data": ("synthetic (seeded complex-Gaussian singlet start vector; operator from the reference's physics)"
+                     if a.start == "seeded" else
+                     "synthetic operator from the reference's physics; start block from the reference's initial guess"),
+            "config": {"workload": a.workload, "start": a.start,
+                       "N": w["n"], "NN": nn, "dim": dim, "nev": w["nev"], "ns": w["ns"],
                        "order": w["order"], "theta": w["theta"], "delta": w["delta"], "sigma": w["sigma"],
                        "tol": w["tol"], "precision": a.precision,
                        "l2": "inputs larger than L2 (GPLMR workspace "
