@@ -40,6 +40,7 @@
 #include <cstring>
 
 #include "de_internal.h"
+#include "gmres.h"
 
 using namespace de;
 
@@ -674,104 +675,81 @@ struct Solver {
         return DE_OK;
     }
 
-    // PRECBLOCK_PETSC gplmr.F90:507-563: b_j <- GMRES solution of
-    // (H - shift) x = b_j, column by column, in the configuration PETSCSOLVE
-    // petscsolve.F90:142-279 gives KSPGMRES.  PETSc's defaults apply: restart
-    // 30, classical Gram-Schmidt without refinement (one Gram of the basis
-    // against w, then one update), no preconditioner (GM_PCOPT = 0 on a shell
-    // operator), zero initial guess.  KSPSetTolerances sets rtol = GM_TOL and
-    // max_it = GM_MAX_INNER_ITER; the default test stops when the Arnoldi
-    // residual estimate |g_{k+1}| <= max(rtol ||b||, 1e-50), or at a happy
-    // breakdown.  The shift is the reference's GMSOLVER%SHIFT, which nothing
-    // assigns: its main-program storage is zero, so the operator is H.
-    int gmres_col(double2 *b)
-    {
-        const int max_it = gm.max_inner_iter;
-        const int mk = std::min(max_it, kGmresRestart);
-        double2 *V = GV, *xg = GV + (int64_t)(mk + 1) * D, *r = xg + D;
-        double2 *dn2 = dGs + 64, *dy = dGs + 80;
-        double bn2 = 0.0;
-        DE_TRY(sqnorm(b, dn2, &bn2));
-        const double bnorm = std::sqrt(bn2), ttol = std::max(gm.tol * bnorm, 1e-50);
-        if (bnorm <= ttol) {  // converged at iteration 0: x = 0
-            DE_CUDA(cudaMemsetAsync(b, 0, D * sizeof(double2), st));
+    // Device operations of gmres_run (gmres.h) on one column b, with the
+    // basis V, iterate xg and residual r in GV, and device scalars in dGs.
+    struct GmresDev {
+        Solver &S;
+        double2 *b, *V, *xg, *r, *dn2, *dy;
+
+        int sqnorm_b(double &n2) { return S.sqnorm(b, dn2, &n2); }
+        int sqnorm_r(double &n2) { return S.sqnorm(r, dn2, &n2); }
+        int copy_b_to_r()
+        {
+            DE_CUDA(cudaMemcpyAsync(r, b, S.D * sizeof(double2), cudaMemcpyDeviceToDevice, S.st));
             return DE_OK;
         }
-        DE_CUDA(cudaMemcpyAsync(r, b, D * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-        int its = 0;
-        bool first = true, done = false;
-        double beta2 = bn2;
-        std::vector<cplx> hh((size_t)(mk + 1) * mk), g(mk + 1), cs(mk), sn(mk), c(mk + 1);
-        while (!done) {
-            if (!first) DE_TRY(sqnorm(r, dn2, &beta2));
-            DE_CUDA(cudaMemcpyAsync(V, r, D * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-            DE_TRY(scale_by_inv_norm(V, dn2));
-            std::fill(g.begin(), g.end(), cplx(0.0));
-            g[0] = std::sqrt(beta2);
-            int k = 0;
-            while (k < mk && its < max_it) {
-                double2 *w = col(V, k + 1);
-                DE_TRY(matblock(col(V, k), w, 1));
-                DE_TRY(gram_dev(cols(V, k + 1, D), cols(w, 1, D), dGs, k + 1));
-                DE_TRY(update(cl(V, k + 1), {w}, dGs, k + 1, -1.0, 1.0));
-                const double2 *a[1] = {w};
-                cudaError_t e = dotdiag_launch(a, a, 1, D, 1, dn2, h->d_work, st);
-                if (e != cudaSuccess) return cuda_error(e, "dotdiag");
-                DE_CUDA(cudaMemcpyAsync(hbuf, dGs, 65 * sizeof(double2), cudaMemcpyDeviceToHost, st));
-                DE_CUDA(cudaStreamSynchronize(st));
-                const double tt = std::sqrt(hbuf[64].x);
-                for (int i = 0; i <= k; ++i) c[i] = cplx(hbuf[i].x, hbuf[i].y);
-                c[k + 1] = tt;
-                for (int i = 0; i < k; ++i) {  // earlier rotations
-                    const cplx a0 = c[i], a1 = c[i + 1];
-                    c[i] = std::conj(cs[i]) * a0 + sn[i] * a1;
-                    c[i + 1] = -std::conj(sn[i]) * a0 + cs[i] * a1;
-                }
-                const double hapbnd = std::min(g[k] != 0.0 ? std::abs(tt / g[k]) : 1e-30, 1e-30);
-                const bool hap = tt < hapbnd;
-                const double den = std::sqrt(std::norm(c[k]) + std::norm(c[k + 1]));
-                ++its;
-                if (den == 0.0) {  // KSP_DIVERGED_NULL: keep the earlier columns
-                    done = true;
-                    break;
-                }
-                cs[k] = c[k] / den;
-                sn[k] = c[k + 1] / den;
-                c[k] = den;
-                c[k + 1] = 0.0;
-                g[k + 1] = -std::conj(sn[k]) * g[k];
-                g[k] = std::conj(cs[k]) * g[k];
-                for (int i = 0; i <= k + 1; ++i) hh[i + (size_t)(mk + 1) * k] = c[i];
-                const double res = std::abs(g[k + 1]);
-                ++k;
-                if (res <= ttol || hap || its >= max_it) {
-                    done = true;
-                    break;
-                }
-                DE_TRY(scale_by_inv_norm(w, dn2));
-            }
-            // back substitution R y = g, then x (+)= V y
-            std::vector<cplx> y(k);
-            for (int i = k - 1; i >= 0; --i) {
-                cplx t = g[i];
-                for (int j = i + 1; j < k; ++j) t -= hh[i + (size_t)(mk + 1) * j] * y[j];
-                y[i] = t / hh[i + (size_t)(mk + 1) * i];
-            }
-            if (k > 0) {
-                DE_TRY(upload(y, dy));
-                DE_TRY(update(cl(V, k), {xg}, dy, k, 1.0, first ? 0.0 : 1.0));
-            } else if (first) {
-                DE_CUDA(cudaMemsetAsync(xg, 0, D * sizeof(double2), st));
-            }
-            first = false;
-            if (!done) {  // restart: r = b - (H - shift) x
-                DE_TRY(matblock(xg, r, 1));
-                cudaError_t e = axpy_launch(r, b, r, make_double2(-1.0, 0.0), D, st);
-                if (e != cudaSuccess) return cuda_error(e, "axpy");
-            }
+        int r_to_v0()
+        {
+            DE_CUDA(cudaMemcpyAsync(V, r, S.D * sizeof(double2), cudaMemcpyDeviceToDevice, S.st));
+            return S.scale_by_inv_norm(V, dn2);
         }
-        DE_CUDA(cudaMemcpyAsync(b, xg, D * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-        return DE_OK;
+        int arnoldi(int k, cplx *coef, double &tt)
+        {
+            double2 *w = S.col(V, k + 1);
+            DE_TRY(S.matblock(S.col(V, k), w, 1));
+            DE_TRY(S.gram_dev(cols(V, k + 1, S.D), cols(w, 1, S.D), S.dGs, k + 1));
+            DE_TRY(S.update(S.cl(V, k + 1), {w}, S.dGs, k + 1, -1.0, 1.0));
+            const double2 *a[1] = {w};
+            cudaError_t e = dotdiag_launch(a, a, 1, S.D, 1, dn2, S.h->d_work, S.st);
+            if (e != cudaSuccess) return cuda_error(e, "dotdiag");
+            DE_CUDA(cudaMemcpyAsync(S.hbuf, S.dGs, 65 * sizeof(double2), cudaMemcpyDeviceToHost, S.st));
+            DE_CUDA(cudaStreamSynchronize(S.st));
+            tt = std::sqrt(S.hbuf[64].x);
+            for (int i = 0; i <= k; ++i) coef[i] = cplx(S.hbuf[i].x, S.hbuf[i].y);
+            return DE_OK;
+        }
+        int normalize_v(int k) { return S.scale_by_inv_norm(S.col(V, k), dn2); }
+        int set_x(const std::vector<cplx> &y, int k, bool accumulate)
+        {
+            DE_TRY(S.upload(y, dy));
+            return S.update(S.cl(V, k), {xg}, dy, k, 1.0, accumulate ? 1.0 : 0.0);
+        }
+        int zero_x()
+        {
+            DE_CUDA(cudaMemsetAsync(xg, 0, S.D * sizeof(double2), S.st));
+            return DE_OK;
+        }
+        int zero_result()
+        {
+            DE_CUDA(cudaMemsetAsync(b, 0, S.D * sizeof(double2), S.st));
+            return DE_OK;
+        }
+        int residual()  // r = b - (H - shift) x, the shift being zero
+        {
+            DE_TRY(S.matblock(xg, r, 1));
+            cudaError_t e = axpy_launch(r, b, r, make_double2(-1.0, 0.0), S.D, S.st);
+            if (e != cudaSuccess) return cuda_error(e, "axpy");
+            return DE_OK;
+        }
+        int x_to_result()
+        {
+            DE_CUDA(cudaMemcpyAsync(b, xg, S.D * sizeof(double2), cudaMemcpyDeviceToDevice, S.st));
+            return DE_OK;
+        }
+    };
+
+    // PRECBLOCK_PETSC gplmr.F90:507-563: b <- the GMRES solution of
+    // (H - shift) x = b (gmres.h: KSPGMRES as PETSCSOLVE petscsolve.F90:142-279
+    // configures it).  The shift is the reference's GMSOLVER%SHIFT, which
+    // nothing assigns: its main-program storage is zero, so the operator is H.
+    // Each iteration is one matvec, one Gram of the basis against the new
+    // vector, one update and one norm, with one host sync for the rotation.
+    int gmres_col(double2 *b)
+    {
+        const int mk = std::min(gm.max_inner_iter, kGmresRestart);
+        GmresDev o{*this, b, GV, GV + (int64_t)(mk + 1) * D, GV + (int64_t)(mk + 2) * D, dGs + 64, dGs + 80};
+        int its = 0;
+        return gmres_run(o, gm.max_inner_iter, gm.tol, kGmresRestart, &its);
     }
 
     // PRECBLOCK gplmr.F90:466-502 (in place)
