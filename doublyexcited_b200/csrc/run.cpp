@@ -53,6 +53,13 @@ extern "C" DE_API int de_run(const de_input *in, int verbose, de_complex *e, de_
         totget = std::min(maxget, nev + skip + 5);
     }
     if (totget > 16) return set_error(DE_E_INVALID, "TOTGET %d exceeds the 16 start vectors supported", totget);
+    if (in->readvecs) {  // the file is checked before any GPU work
+        int64_t fm = 0;
+        int fnum = 0;
+        DE_TRY(de_vectors_header(in->invecfile, &fm, &fnum));
+        if (fnum < totget)
+            return set_error(DE_E_IO, "%s holds %d vectors, %d requested", in->invecfile, fnum, totget);
+    }
 
     Owned P;
     DE_TRY(de_problem_create(&in->params, &P.h));

@@ -44,3 +44,18 @@ def test_command_line_reports_input_errors(tmp_path):
                        env={**os.environ, "PYTHONPATH": root})
     assert p.returncode == 1  # DE_E_INVALID
     assert "TOO BIG FOR NUMORBS" in p.stderr and "Traceback" not in p.stderr
+
+
+def test_run_checks_the_vector_file_before_gpu_work(de, tmp_path):
+    """READVECS: a missing file, or one with fewer vectors than NEV+NUMSKIP,
+    is an I/O error before the operator is built."""
+    import numpy as np
+
+    with pytest.raises(de.DeError) as e:
+        de.run(["N=2", "Read", "Nev=1", f"Infile='{tmp_path / 'absent'}'"], path=str(tmp_path / "absent.inp"))
+    assert e.value.status == de.DE_E_IO
+    f = tmp_path / "one"
+    de.write_vectors(str(f), np.zeros((5 ** 6, 1), np.complex128), 5 ** 3)
+    with pytest.raises(de.DeError) as e:
+        de.run(["N=2", "Read", "Nev=2", f"Infile='{f}'"], path=str(tmp_path / "absent.inp"))
+    assert e.value.status == de.DE_E_IO and "holds 1 vectors, 2 requested" in str(e.value)
