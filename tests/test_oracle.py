@@ -113,8 +113,9 @@ def test_oracle_gplmr_small_runs(oracle):
 
 def test_subspace_guess_matches_reference_log(oracle):
     """The initial guess at N=5 (14 He+ orbitals, singlet products, c-product
-    subspace): the six subspace eigenvalues nearest the shift equal those the
-    reference printed (Out.S.N5:100-107) to the accuracy of its Lanczos
+    subspace): the six subspace eigenvalues nearest the shift, their
+    expectation values and the chosen shift equal those the reference printed
+    (Out.S.N5:100-116) to the accuracy of its Lanczos
     orbitals (error 1.8e-3 at Out.S.N5:48).  With exact orbitals the 2p-like
     triple is exactly degenerate; the reference's is split by ~1e-5."""
     p = oracle.Params(n=5, delta=2.0, theta=0.2)
@@ -138,6 +139,17 @@ def test_subspace_guess_matches_reference_log(oracle):
         assert np.max(np.abs(xm - xm.T)) < 1e-12
     hx = h2.matvec(x[:, 0])
     assert abs(np.dot(x[:, 0], hx) / np.dot(x[:, 0], x[:, 0]) - e0[0]) < 1e-10
+    # GET_EXPECTS on the guess (Hermitian Rayleigh quotients, Out.S.N5:108-115)
+    # and the shift rule: CHOSEN SHIFT = mean of the first NEV = 1 values, its
+    # imaginary part kept in that run (Out.S.N5:116)
+    ex = oracle.get_expects(h2, x)
+    ex_log = [(-0.71103418289003, 0.03135694997228), (-0.63342042390045, 0.03098376935548),
+              (-0.63341526129029, 0.03097755505683), (-0.63340345447343, 0.03098181163344),
+              (-0.62578990443867, 0.02731929431511), (-0.62579224777072, 0.02732108826907)]
+    ex_log = np.array([complex(a, b) for a, b in ex_log])
+    assert abs(ex[0] - ex_log[0]) < 5e-6
+    assert np.max(np.abs(ex - ex_log)) < 2e-5
+    assert abs(oracle.gplmr_shift(ex, 1, takerealpart=False) - complex(-0.7110341829, 0.0313569500)) < 5e-6
 
 
 def _krylov_minimizer(a, b, k):
