@@ -641,6 +641,20 @@ def get_expects(h: Hamiltonian, psi: np.ndarray, cshiftopt: bool = False) -> np.
     return np.array(out)
 
 
+def sixd_fix(x: np.ndarray, n_in: int, n_out: int) -> np.ndarray:
+    """SIXD_FIX utils.F90:186-198: a two-electron vector on the (2 n_in + 1)^6
+    grid copied onto the (2 n_out + 1)^6 grid about the centre, cropped or
+    zero-padded in all six indices (column-major, electron 1 fastest)."""
+    a, b = 2 * n_in + 1, 2 * n_out + 1
+    v = np.asarray(x, np.complex128).reshape((a,) * 6, order="F")
+    out = np.zeros((b,) * 6, np.complex128, order="F")
+    k = min(n_in, n_out)
+    si = slice(n_in - k, n_in + k + 1)
+    so = slice(n_out - k, n_out + k + 1)
+    out[(so,) * 6] = v[(si,) * 6]
+    return out.reshape(-1, order="F")
+
+
 def gplmr_shift(expects: np.ndarray, nev: int, takerealpart: bool = True) -> complex:
     """doublyexcited.F90:214-219."""
     s = complex(np.sum(expects[:nev]) / nev)

@@ -206,3 +206,14 @@ def test_gmres_and_basic_inner_solves_find_the_same_resonance():
     b = load_json("gplmr_n3_nev1.json")
     assert a["solver"]["usepetscflag"] == 0
     assert abs(complex(*a["e"][0]) - complex(*b["e"][0])) < 1e-10
+
+
+@pytest.mark.parametrize("n_in,n_out", [(2, 3), (3, 2), (2, 2)])
+def test_sixd_fix_matches_the_library_reader(de, oracle, tmp_path, n_in, n_out):
+    """The oracle's SIXD_FIX (utils.F90:186-198) and de_read_vectors reading a
+    file written for another grid resize a vector identically."""
+    x = oracle.seeded_vectors((2 * n_in + 1) ** 6, 1, 5)[:, 0]
+    f = tmp_path / "v"
+    de.write_vectors(str(f), x.reshape(-1, 1), (2 * n_in + 1) ** 3)
+    y = de.read_vectors(str(f), (2 * n_out + 1) ** 3, 1)[:, 0]
+    assert np.array_equal(y, oracle.sixd_fix(x, n_in, n_out))
