@@ -124,6 +124,40 @@ def gplmr_fixture(n, theta, sigma, nev, compat, maxit, tol, seed=0, spin="single
     }
 
 
+def pipeline_n5_petsc():
+    """PROGRAM ATOM at N=5 as the reference's logged run (Out.S.N5) made it:
+    14 He+ orbitals, singlet products, TOTGET 6, the shift = the first
+    expectation value with its imaginary part kept, then GPLMR with
+    gm_usepetscflag = 0 (the PETSc GMRES path), order 5, tol 1e-7."""
+    p = O.Params(n=5, delta=2.0, theta=0.2)
+    h1 = O.init_hamiltonian(p, nelec=1)
+    h2 = O.init_hamiltonian(p, nelec=2)
+    t0 = time.time()
+    _, v = O.heplus_orbitals(h1, 14)
+    ev = O.orbital_gather(v)
+    e0, x, _ = O.diagsubspace(h2, ev, True, False, complex(-0.7131541429, 0), 6)
+    ex = O.get_expects(h2, x)
+    sigma = O.gplmr_shift(ex, 1, takerealpart=False)
+    c0 = h2.calls
+    r = O.gplmr_eig(h2, x[:, :1], sigma, ns=5, maxit=40, tol=1e-7, order=5, usepetscflag=0, gm_tol=1e-3)
+    return {
+        "params": {"n": 5, "delta": 2.0, "theta": 0.2, "charge": 2.0},
+        "guess": {"numorbs": 14, "singlet": True, "hermopt": False, "etarget": _c(-0.7131541429), "totget": 6},
+        "solver": {"ns": 5, "order": 5, "maxit": 40, "tol": 1e-7, "usepetscflag": 0, "gm_tol": 1e-3,
+                   "takerealpart": False},
+        "e0": [_c(z) for z in e0], "expects": [_c(z) for z in ex], "shift": _c(sigma),
+        "iterations": r.iterations, "matvecs_gplmr": h2.calls - c0,
+        "e": [_c(z) for z in r.e], "residuals": [float(v) for v in r.residuals],
+        "history": [{"it": it, "e": [_c(z) for z in e], "res": [float(v) for v in res]} for it, e, res in r.history],
+        "reference_log": {"source": "CSCALE-WORK/Outs/Out.S.N5:116-147",
+                          "shift": [-0.7110341829, 0.0313569500],
+                          "it10": {"e": [-0.713201879088, 0.035040828161], "err": 8.84e-4},
+                          "it20": {"e": [-0.713154201184, 0.035226942020], "err": 4.10e-6},
+                          "final": {"it": 29, "e": [-0.713154142874, 0.035227459486], "err": 7.99e-8}},
+        "oracle_seconds": time.time() - t0,
+    }
+
+
 FIXTURES = {
     "heplus_n5": (False, lambda: ("json", heplus_n5())),
     "hammult_n1": (False, lambda: ("npz", hammult_fixture(1, 0.3, 11, True))),
@@ -140,6 +174,7 @@ FIXTURES = {
                                                                  usepetscflag=0))),
     "gplmr_n3_nev2_petsc": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 2, False, 6, 1e-10,
                                                                  usepetscflag=0))),
+    "pipeline_n5_petsc": (True, lambda: ("json", pipeline_n5_petsc())),
     "gplmr_n5_nev1": (True, lambda: ("json", gplmr_fixture(5, 0.2, complex(-0.7131541429, 0), 1, False, 60, 1e-9))),
     "gplmr_n6_nev1": (True, lambda: ("json", gplmr_fixture(6, 0.2, complex(-0.7131541429, 0), 1, False, 80, 1e-8))),
 }

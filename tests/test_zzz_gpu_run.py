@@ -8,6 +8,8 @@ suite stops at its first failure and this test is the newest.)"""
 import numpy as np
 import pytest
 
+from conftest import load_json
+
 pytestmark = pytest.mark.gpu
 
 
@@ -33,3 +35,26 @@ def test_run_replays_the_program_step_by_step(de, tmp_path):
     assert abs(r.e[0] - g.e[0]) < 1e-10
     back = de.read_vectors(str(out), 7 ** 3, 1)
     assert np.array_equal(back[:, 0], r.x[:, 0])
+
+
+def test_run_replays_the_reference_n5_program(de, tmp_path):
+    """The reference's logged N=5 run (Out.S.N5) through de_run with its
+    settings: 14 orbitals, singlet, NEV 1, the shift's imaginary part kept,
+    gm_usepetscflag = 0 (the PETSc GMRES path), tol 1e-7.  Against the
+    oracle's replay of the same program (pipeline_n5_petsc.json): the shift
+    to 1e-9, the iteration count to one (the last residual sits near the
+    tolerance), the resonance to 2e-8 Hartree; and the logged resonance to
+    3e-8 (its start came from Lanczos orbitals)."""
+    g = load_json("pipeline_n5_petsc.json")
+    inp = tmp_path / "Input.Inp"
+    inp.write_text("&grid\n AUTODELTA=.false.\n DELTA=2d0\n N=5\n/\n"
+                   "&orbitals\n NUMORBS=14\n SINGLET=T\n/\n"
+                   "&gmres\n gm_usepetscflag=0\n/\n"
+                   "&gplmr\n GPLMR_SHIFT=(-0.7131541429d0,0d0)\n GPLMR_MAXIT=40\n GPLMR_TOL=1D-7\n"
+                   " GPLMR_NEV=1\n TAKEREALPART=.FALSE.\n/\n")
+    r = de.run([f"Inp={inp}", "Theta=0.2"])
+    assert r.totget == 6
+    assert abs(r.shift - complex(*g["shift"])) < 1e-9
+    assert r.converged and abs(r.iterations - g["iterations"]) <= 1
+    assert abs(r.e[0] - complex(*g["e"][0])) < 2e-8
+    assert abs(r.e[0] - complex(*g["reference_log"]["final"]["e"])) < 3e-8
