@@ -158,6 +158,48 @@ def pipeline_n5_petsc():
     }
 
 
+def pipeline_n6_readvecs():
+    """The reference's N=6 runs (Out.S.D2d0.T0.2d0.N6.petsc / .nopetsc): READVECS
+    of the converged N=5 eigenvector (the N=5 program above), SIXD_FIX onto
+    the N=6 grid, the shift = the real part of its expectation value, then
+    GPLMR to 1e-7 with gm_usepetscflag = 1 (BASIC) and = 0 (GMRES)."""
+    t0 = time.time()
+    p5 = O.Params(n=5, delta=2.0, theta=0.2)
+    h1 = O.init_hamiltonian(p5, nelec=1)
+    h5 = O.init_hamiltonian(p5, nelec=2)
+    _, v = O.heplus_orbitals(h1, 14)
+    e0, x, _ = O.diagsubspace(h5, O.orbital_gather(v), True, False, complex(-0.7131541429, 0), 6)
+    sigma5 = O.gplmr_shift(O.get_expects(h5, x), 1, takerealpart=False)
+    r5 = O.gplmr_eig(h5, x[:, :1], sigma5, ns=5, maxit=40, tol=1e-7, order=5, usepetscflag=0, gm_tol=1e-3)
+    del h5
+    p6 = O.Params(n=6, delta=2.0, theta=0.2)
+    h6 = O.init_hamiltonian(p6, nelec=2)
+    x6 = O.sixd_fix(r5.x[:, 0], 5, 6).reshape(-1, 1)
+    ex = O.get_expects(h6, x6)
+    sigma = O.gplmr_shift(ex, 1, takerealpart=True)
+    runs = {}
+    for flag in (1, 0):
+        r = O.gplmr_eig(h6, x6, sigma, ns=5, maxit=40, tol=1e-7, order=5, usepetscflag=flag, gm_tol=1e-3)
+        runs[str(flag)] = {"iterations": r.iterations, "e": [_c(z) for z in r.e],
+                           "history": [{"it": it, "e": [_c(z) for z in e], "res": [float(q) for q in res]}
+                                       for it, e, res in r.history]}
+    return {
+        "params": {"n": 6, "delta": 2.0, "theta": 0.2, "charge": 2.0},
+        "start": {"kind": "sixd_fix of the N=5 program's eigenvector", "n5_iterations": r5.iterations,
+                  "n5_e": _c(r5.e[0])},
+        "expects": _c(ex[0]), "shift": _c(sigma), "runs_by_usepetscflag": runs,
+        "reference_log": {
+            "expects": [-0.71315414287425, 0.03522745948576],
+            "1": {"source": "CSCALE-WORK/Outs/Out.S.D2d0.T0.2d0.N6.petsc:67-97",
+                  "it10": {"e": [-0.713140739245, 0.035275491290], "err": 2.21e-6},
+                  "final": {"it": 16, "e": [-0.713140520365, 0.035275084711], "err": 5.65e-8}},
+            "0": {"source": "CSCALE-WORK/Outs/Out.S.D2d0.T0.2d0.N6.nopetsc:67-96",
+                  "it10": {"e": [-0.713142523131, 0.035276034752], "err": 1.07e-5},
+                  "final": {"it": 20, "e": [-0.713140523217, 0.035275093419], "err": 8.32e-8}}},
+        "oracle_seconds": time.time() - t0,
+    }
+
+
 FIXTURES = {
     "heplus_n5": (False, lambda: ("json", heplus_n5())),
     "hammult_n1": (False, lambda: ("npz", hammult_fixture(1, 0.3, 11, True))),
@@ -175,6 +217,7 @@ FIXTURES = {
     "gplmr_n3_nev2_petsc": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 2, False, 6, 1e-10,
                                                                  usepetscflag=0))),
     "pipeline_n5_petsc": (True, lambda: ("json", pipeline_n5_petsc())),
+    "pipeline_n6_readvecs": (True, lambda: ("json", pipeline_n6_readvecs())),
     "gplmr_n5_nev1": (True, lambda: ("json", gplmr_fixture(5, 0.2, complex(-0.7131541429, 0), 1, False, 60, 1e-9))),
     "gplmr_n6_nev1": (True, lambda: ("json", gplmr_fixture(6, 0.2, complex(-0.7131541429, 0), 1, False, 80, 1e-8))),
 }

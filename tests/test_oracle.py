@@ -240,3 +240,24 @@ def test_gmres_pipeline_reproduces_the_reference_n5_run():
     # ICALLED: 6 MATBLOCK products and 6 PETSc solves of 5 GMRES iterations
     # per GPLMR iteration, as the log's counter shows
     assert g["matvecs_gplmr"] == 1 + 36 * g["iterations"]
+
+
+def test_readvecs_pipeline_reproduces_the_reference_n6_runs():
+    """The reference's N=6 runs read the N=5 eigenvector onto the bigger grid
+    (SIXD_FIX), take the real part of its expectation value as the shift and
+    solve with BASIC (Out.S.D2d0.T0.2d0.N6.petsc, flag 1) or GMRES
+    (.nopetsc, flag 0).  The oracle's replay (pipeline_n6_readvecs.json)
+    matches the expectation value, the converged resonance and the iteration
+    count of both.  Its start is the oracle's own N=5 eigenvector, converged
+    to the same 1e-7 residual as the reference's, so mid-run residuals agree
+    within a factor of 2."""
+    g = load_json("pipeline_n6_readvecs.json")
+    log = g["reference_log"]
+    assert abs(complex(*g["expects"]) - complex(*log["expects"])) < 3e-8
+    for flag in ("1", "0"):
+        run, ref = g["runs_by_usepetscflag"][flag], log[flag]
+        h10 = {h["it"]: h for h in run["history"]}[10]
+        assert 0.5 < h10["res"][0] / ref["it10"]["err"] < 2.0
+        assert abs(complex(*h10["e"][0]) - complex(*ref["it10"]["e"])) < 1e-6
+        assert abs(run["iterations"] - ref["final"]["it"]) <= 1
+        assert abs(complex(*run["e"][0]) - complex(*ref["final"]["e"])) < 3e-8

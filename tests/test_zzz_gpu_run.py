@@ -58,3 +58,31 @@ def test_run_replays_the_reference_n5_program(de, tmp_path):
     assert r.converged and abs(r.iterations - g["iterations"]) <= 1
     assert abs(r.e[0] - complex(*g["e"][0])) < 2e-8
     assert abs(r.e[0] - complex(*g["reference_log"]["final"]["e"])) < 3e-8
+
+
+def test_run_warm_starts_n6_from_the_n5_eigenvector(de, tmp_path):
+    """The reference's warm start along N (Out.S.N5 then
+    Out.S.D2d0.T0.2d0.N6.petsc): the N=5 program writes its eigenvector, the
+    N=6 program reads it onto the bigger grid (SIXD_FIX), takes the real part
+    of its expectation value as the shift and solves on the BASIC path
+    (gm_usepetscflag = 1).  Against the oracle's replay
+    (pipeline_n6_readvecs.json) and the logged resonance."""
+    g = load_json("pipeline_n6_readvecs.json")
+    vec = tmp_path / "eigvecs.S.N5"
+    inp5 = tmp_path / "Input.N5"
+    inp5.write_text("&main\n WRITEVECS=.TRUE.\n/\n&grid\n AUTODELTA=.false.\n DELTA=2d0\n N=5\n/\n"
+                    "&orbitals\n NUMORBS=14\n SINGLET=T\n/\n&gmres\n gm_usepetscflag=0\n/\n"
+                    "&gplmr\n GPLMR_SHIFT=(-0.7131541429d0,0d0)\n GPLMR_MAXIT=40\n GPLMR_TOL=1D-7\n"
+                    " GPLMR_NEV=1\n TAKEREALPART=.FALSE.\n/\n")
+    r5 = de.run([f"Inp={inp5}", "Theta=0.2", f"Outfile='{vec}'"])
+    assert r5.converged
+    inp6 = tmp_path / "Input.N6"
+    inp6.write_text("&grid\n AUTODELTA=.false.\n DELTA=2d0\n/\n&gmres\n gm_usepetscflag=1\n/\n"
+                    "&gplmr\n GPLMR_MAXIT=40\n GPLMR_TOL=1D-7\n GPLMR_NEV=1\n/\n")
+    r6 = de.run([f"Inp={inp6}", "Read", "N=6", "Theta=0.2", f"Infile='{vec}'"])
+    run, log = g["runs_by_usepetscflag"]["1"], g["reference_log"]
+    assert r6.totget == 1
+    assert abs(r6.expects[0] - complex(*g["expects"])) < 3e-8
+    assert r6.converged and abs(r6.iterations - run["iterations"]) <= 1
+    assert abs(r6.e[0] - complex(*run["e"][0])) < 3e-8
+    assert abs(r6.e[0] - complex(*log["1"]["final"]["e"])) < 4e-8
