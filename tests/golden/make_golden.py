@@ -200,6 +200,36 @@ def pipeline_n6_readvecs():
     }
 
 
+def pipeline_n6_readvecs_order20():
+    """The reference's N=6 BASIC run at inner order 20
+    (Out.S.D2d0.T0.2d0.N6.petsc.20_inner_iter): the warm start of
+    pipeline_n6_readvecs, GPLMR to 1e-7 with gm_max_inner_iter = 20."""
+    t0 = time.time()
+    p5 = O.Params(n=5, delta=2.0, theta=0.2)
+    h1 = O.init_hamiltonian(p5, nelec=1)
+    h5 = O.init_hamiltonian(p5, nelec=2)
+    _, v = O.heplus_orbitals(h1, 14)
+    e0, x, _ = O.diagsubspace(h5, O.orbital_gather(v), True, False, complex(-0.7131541429, 0), 6)
+    sigma5 = O.gplmr_shift(O.get_expects(h5, x), 1, takerealpart=False)
+    r5 = O.gplmr_eig(h5, x[:, :1], sigma5, ns=5, maxit=40, tol=1e-7, order=5, usepetscflag=0, gm_tol=1e-3)
+    del h5
+    h6 = O.init_hamiltonian(O.Params(n=6, delta=2.0, theta=0.2), nelec=2)
+    x6 = O.sixd_fix(r5.x[:, 0], 5, 6).reshape(-1, 1)
+    sigma = O.gplmr_shift(O.get_expects(h6, x6), 1, takerealpart=True)
+    c0 = h6.calls
+    r = O.gplmr_eig(h6, x6, sigma, ns=5, maxit=40, tol=1e-7, order=20, usepetscflag=1)
+    return {
+        "params": {"n": 6, "delta": 2.0, "theta": 0.2, "charge": 2.0},
+        "solver": {"ns": 5, "order": 20, "tol": 1e-7, "usepetscflag": 1},
+        "shift": _c(sigma), "iterations": r.iterations, "matvecs_gplmr": h6.calls - c0,
+        "e": [_c(z) for z in r.e],
+        "history": [{"it": it, "e": [_c(z) for z in e], "res": [float(q) for q in res]} for it, e, res in r.history],
+        "reference_log": {"source": "CSCALE-WORK/Outs/Out.S.D2d0.T0.2d0.N6.petsc.20_inner_iter:67-96",
+                          "final": {"it": 6, "e": [-0.713140520817, 0.035275088028], "err": 1.82e-8}},
+        "oracle_seconds": time.time() - t0,
+    }
+
+
 FIXTURES = {
     "heplus_n5": (False, lambda: ("json", heplus_n5())),
     "hammult_n1": (False, lambda: ("npz", hammult_fixture(1, 0.3, 11, True))),
@@ -218,6 +248,7 @@ FIXTURES = {
                                                                  usepetscflag=0))),
     "pipeline_n5_petsc": (True, lambda: ("json", pipeline_n5_petsc())),
     "pipeline_n6_readvecs": (True, lambda: ("json", pipeline_n6_readvecs())),
+    "pipeline_n6_readvecs_order20": (True, lambda: ("json", pipeline_n6_readvecs_order20())),
     "gplmr_n5_nev1": (True, lambda: ("json", gplmr_fixture(5, 0.2, complex(-0.7131541429, 0), 1, False, 60, 1e-9))),
     "gplmr_n6_nev1": (True, lambda: ("json", gplmr_fixture(6, 0.2, complex(-0.7131541429, 0), 1, False, 80, 1e-8))),
 }

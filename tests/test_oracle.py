@@ -261,3 +261,17 @@ def test_readvecs_pipeline_reproduces_the_reference_n6_runs():
         assert abs(complex(*h10["e"][0]) - complex(*ref["it10"]["e"])) < 1e-6
         assert abs(run["iterations"] - ref["final"]["it"]) <= 1
         assert abs(complex(*run["e"][0]) - complex(*ref["final"]["e"])) < 3e-8
+
+
+def test_order20_basic_run_reproduces_the_reference_n6_log():
+    """BASIC at inner order 20 from the same warm start
+    (Out.S.D2d0.T0.2d0.N6.petsc.20_inner_iter): the oracle converges at the
+    logged iteration 6, residual 1.9e-8 against the logged 1.82e-8, resonance
+    within 3e-10 of the log, and 1 + 6 (1 + NS)(1 + 2*20 + 1) products as the
+    log's ICALLED counter shows."""
+    g = load_json("pipeline_n6_readvecs_order20.json")
+    ref = g["reference_log"]["final"]
+    assert g["iterations"] == ref["it"]
+    assert 0.5 < g["history"][-1]["res"][0] / ref["err"] < 2.0
+    assert abs(complex(*g["e"][0]) - complex(*ref["e"])) < 1e-9
+    assert g["matvecs_gplmr"] == 1 + g["iterations"] * 6 * 42

@@ -86,3 +86,26 @@ def test_run_warm_starts_n6_from_the_n5_eigenvector(de, tmp_path):
     assert r6.converged and abs(r6.iterations - run["iterations"]) <= 1
     assert abs(r6.e[0] - complex(*run["e"][0])) < 3e-8
     assert abs(r6.e[0] - complex(*log["1"]["final"]["e"])) < 4e-8
+
+
+def test_run_warm_start_at_inner_order_20(de, tmp_path):
+    """Out.S.D2d0.T0.2d0.N6.petsc.20_inner_iter: the same warm start with
+    BASIC at inner order 20 (Iter=20), which also takes the inner solve's
+    Gram-Schmidt past 16 earlier vectors.  Against the oracle's replay
+    (pipeline_n6_readvecs_order20.json) and the logged resonance.  Kept last:
+    it is the one GPU test of an inner order above 16."""
+    g = load_json("pipeline_n6_readvecs_order20.json")
+    vec = tmp_path / "eigvecs.S.N5"
+    inp5 = tmp_path / "Input.N5"
+    inp5.write_text("&main\n WRITEVECS=.TRUE.\n/\n&grid\n AUTODELTA=.false.\n DELTA=2d0\n N=5\n/\n"
+                    "&orbitals\n NUMORBS=14\n SINGLET=T\n/\n&gmres\n gm_usepetscflag=0\n/\n"
+                    "&gplmr\n GPLMR_SHIFT=(-0.7131541429d0,0d0)\n GPLMR_MAXIT=40\n GPLMR_TOL=1D-7\n"
+                    " GPLMR_NEV=1\n TAKEREALPART=.FALSE.\n/\n")
+    assert de.run([f"Inp={inp5}", "Theta=0.2", f"Outfile='{vec}'"]).converged
+    inp6 = tmp_path / "Input.N6"
+    inp6.write_text("&grid\n AUTODELTA=.false.\n DELTA=2d0\n/\n&gmres\n gm_usepetscflag=1\n/\n"
+                    "&gplmr\n GPLMR_MAXIT=40\n GPLMR_TOL=1D-7\n GPLMR_NEV=1\n/\n")
+    r = de.run([f"Inp={inp6}", "Read", "N=6", "Theta=0.2", f"Infile='{vec}'", "Iter=20"])
+    assert r.converged and abs(r.iterations - g["iterations"]) <= 1
+    assert abs(r.e[0] - complex(*g["e"][0])) < 3e-8
+    assert abs(r.e[0] - complex(*g["reference_log"]["final"]["e"])) < 3e-8
