@@ -88,6 +88,33 @@ def test_run_warm_starts_n6_from_the_n5_eigenvector(de, tmp_path):
     assert abs(r6.e[0] - complex(*log["1"]["final"]["e"])) < 4e-8
 
 
+@pytest.mark.parametrize("flag,log_it,log_e", [
+    (1, 17, (-0.713160218513, 0.035265673069)),   # Out.S.D2d0.T0.2d0.N9.petsc:92-98 (BASIC)
+    (0, 22, (-0.713160220730, 0.035265681394)),   # Out.S.D2d0.T0.2d0.N9.nopetsc:92-98 (GMRES)
+])
+def test_run_warm_start_n9_against_the_reference_logs(de, tmp_path, flag, log_it, log_e):
+    """The reference's N=9 runs read the N=5 eigenvector straight onto the
+    19^6 grid.  Their ICALLED counters show 72 products per iteration in
+    the .petsc run (BASIC) and 36 in the .nopetsc run (GMRES).  The same
+    program through de_run, from the N=5 program's eigenvector, against the
+    logs: iteration count within one, resonance within 3e-8 Hartree (both
+    starts are converged only to 1e-7)."""
+    vec = tmp_path / "eigvecs.S.N5"
+    inp5 = tmp_path / "Input.N5"
+    inp5.write_text("&main\n WRITEVECS=.TRUE.\n/\n&grid\n AUTODELTA=.false.\n DELTA=2d0\n N=5\n/\n"
+                    "&orbitals\n NUMORBS=14\n SINGLET=T\n/\n&gmres\n gm_usepetscflag=0\n/\n"
+                    "&gplmr\n GPLMR_SHIFT=(-0.7131541429d0,0d0)\n GPLMR_MAXIT=40\n GPLMR_TOL=1D-7\n"
+                    " GPLMR_NEV=1\n TAKEREALPART=.FALSE.\n/\n")
+    assert de.run([f"Inp={inp5}", "Theta=0.2", f"Outfile='{vec}'"]).converged
+    inp9 = tmp_path / "Input.N9"
+    inp9.write_text(f"&grid\n AUTODELTA=.false.\n DELTA=2d0\n/\n&gmres\n gm_usepetscflag={flag}\n/\n"
+                    "&gplmr\n GPLMR_MAXIT=40\n GPLMR_TOL=1D-7\n GPLMR_NEV=1\n/\n")
+    r = de.run([f"Inp={inp9}", "Read", "N=9", "Theta=0.2", f"Infile='{vec}'"])
+    assert abs(r.expects[0] - complex(-0.71315414287425, 0.03522745948576)) < 3e-8  # Out.S.D2d0.T0.2d0.N9.*:68
+    assert r.converged and abs(r.iterations - log_it) <= 1
+    assert abs(r.e[0] - complex(*log_e)) < 3e-8
+
+
 def test_run_warm_start_at_inner_order_20(de, tmp_path):
     """Out.S.D2d0.T0.2d0.N6.petsc.20_inner_iter: the same warm start with
     BASIC at inner order 20 (Iter=20), which also takes the inner solve's
