@@ -136,3 +136,22 @@ def test_run_warm_start_at_inner_order_20(de, tmp_path):
     assert r.converged and abs(r.iterations - g["iterations"]) <= 1
     assert abs(r.e[0] - complex(*g["e"][0])) < 3e-8
     assert abs(r.e[0] - complex(*g["reference_log"]["final"]["e"])) < 3e-8
+
+
+def test_run_warm_start_n9_at_inner_order_20(de, tmp_path):
+    """Out.S.D2d0.T0.2d0.N9.petsc.120core.20_inner_iter: the N=5 eigenvector
+    read onto N=9, BASIC at inner order 20.  Against the log: converged at
+    iteration 6 (within one), resonance within 3e-8 Hartree (lines 90-96)."""
+    vec = tmp_path / "eigvecs.S.N5"
+    inp5 = tmp_path / "Input.N5"
+    inp5.write_text("&main\n WRITEVECS=.TRUE.\n/\n&grid\n AUTODELTA=.false.\n DELTA=2d0\n N=5\n/\n"
+                    "&orbitals\n NUMORBS=14\n SINGLET=T\n/\n&gmres\n gm_usepetscflag=0\n/\n"
+                    "&gplmr\n GPLMR_SHIFT=(-0.7131541429d0,0d0)\n GPLMR_MAXIT=40\n GPLMR_TOL=1D-7\n"
+                    " GPLMR_NEV=1\n TAKEREALPART=.FALSE.\n/\n")
+    assert de.run([f"Inp={inp5}", "Theta=0.2", f"Outfile='{vec}'"]).converged
+    inp9 = tmp_path / "Input.N9"
+    inp9.write_text("&grid\n AUTODELTA=.false.\n DELTA=2d0\n/\n&gmres\n gm_usepetscflag=1\n/\n"
+                    "&gplmr\n GPLMR_MAXIT=40\n GPLMR_TOL=1D-7\n GPLMR_NEV=1\n/\n")
+    r = de.run([f"Inp={inp9}", "Read", "N=9", "Theta=0.2", f"Infile='{vec}'", "Iter=20"])
+    assert r.converged and abs(r.iterations - 6) <= 1
+    assert abs(r.e[0] - complex(-0.713160212291, 0.035265678863)) < 3e-8
