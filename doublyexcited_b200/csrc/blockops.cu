@@ -18,6 +18,8 @@
 #include "de_internal.h"
 #include "de_kernels.h"
 
+#include <cuda.h>
+
 #include <algorithm>
 #include <atomic>
 #include <mutex>
@@ -440,17 +442,22 @@ __device__ __forceinline__ void reduce_partials(const double2 *__restrict__ part
 template <auto kernel>
 int wave_blocks()
 {
-    static int cache[64] = {};
+    // atomic entries: the handle-free entry point (de_dots_noalloc_d) can
+    // reach this from several host threads at once; every thread computes
+    // the same value, so relaxed order suffices
+    static std::atomic<int> cache[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return 296;
-    if (!cache[dev]) {
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (!v) {
         int sms = 0, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, 0);
-        cache[dev] = std::max(1, sms) * std::max(1, std::min(per, 8));
+        v = std::max(1, sms) * std::max(1, std::min(per, 8));
+        cache[dev].store(v, std::memory_order_relaxed);
     }
-    return cache[dev];
+    return v;
 }
 
 template <auto kernel>
@@ -1466,21 +1473,60 @@ cudaError_t build_tables_launch(int nn, int n, double charge, double delta, cons
 }  // namespace de
 
 // ---------------------------------------------------------------- no-alloc
-// Allocation-free variant of the device dot products, for callers that must
-// not allocate device memory: code recording work into a CUDA graph or
-// running under a pre-reserved memory budget, where a cudaMalloc would break
-// the capture or exceed the reservation.  Its reduction scratch (ticket plus
-// one partial per block and output of the fused small Gram) is a file-scope
-// device array of 1 + 296*32 complex values (151,568 bytes) that every GPU
-// loading this library holds until the process exits.
+// Allocation-free variant of the device dot products, for callers that cannot
+// call cudaMalloc: code embedded in a host application that owns all device
+// memory through its own pool or a fixed reservation (a serving process that
+// reserved its HBM up front), where an allocation from this library would
+// fail or push the process past its reservation.  Its reduction scratch
+// (ticket plus one partial per block and output of the fused small Gram) is
+// a file-scope device array of 1 + 296*32 complex values (151,568 bytes) that
+// every GPU loading this library holds until the process exits.
 
 namespace de {
 
 static __device__ __align__(256) double2 g_dots_scratch[1 + kSmallBlocks * 32];
 
 namespace {
+// The array's device address per device, valid for the context it was looked
+// up in: after cudaDeviceReset (or a released and re-created primary
+// context) the module is loaded again and the address changes, so the
+// cache is keyed on the driver's context id as well.
+struct ScratchAddr {
+    unsigned long long ctx_id;
+    double2 *ptr;
+};
 std::mutex g_scratch_mu;
-double2 *g_scratch_ptr[64] = {};
+ScratchAddr g_scratch_addr[64] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+// Id of the calling thread's current context (0: none current, or the
+// driver offers no id).  The driver entry points come through the runtime,
+// so the library does not link libcuda.
+unsigned long long current_ctx_id()
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 }  // namespace
 
 }  // namespace de
@@ -1505,16 +1551,22 @@ extern "C" DE_API int de_dots_noalloc_d(const de_complex *bras_d, const de_compl
     double2 *scratch = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_scratch_mu);
-        if (!g_scratch_ptr[dev]) {
-            // First call on this device: host code needs the device address of
-            // the array (its host-side symbol is only a stand-in).
-            e = cudaGetSymbolAddress((void **)&g_scratch_ptr[dev], g_dots_scratch);
+        ScratchAddr &a = g_scratch_addr[dev];
+        const unsigned long long id = current_ctx_id();
+        if (!a.ptr || id == 0 || id != a.ctx_id) {
+            // First call on this device (or in a new context of it): host code
+            // needs the device address of the array, whose host-side symbol is
+            // only a stand-in.  This also creates the context if none is
+            // current yet, so the id is read again afterwards.
+            double2 *p = nullptr;
+            e = cudaGetSymbolAddress((void **)&p, g_dots_scratch);
             if (e != cudaSuccess) {
-                g_scratch_ptr[dev] = nullptr;
+                a = ScratchAddr{0, nullptr};
                 return cuda_error(e, "cudaGetSymbolAddress(dots scratch)");
             }
+            a = ScratchAddr{current_ctx_id(), p};
         }
-        scratch = g_scratch_ptr[dev];
+        scratch = a.ptr;
     }
     cudaStream_t st = (cudaStream_t)cuda_stream;
     // the reduction ticket must start at zero whatever the previous call left

@@ -146,10 +146,13 @@ DE_API int de_set_stream(de_problem *h, void *cuda_stream);
  * The reference times phases with MPI_WTIME (gplmr.F90:42-57). */
 DE_API int de_set_profiling(de_problem *h, int on);
 /* Which matvec kernels a handle uses: DE_MATVEC_FMA (the default) the
- * CUDA-core FMA kernels, DE_MATVEC_TENSOR the axis contractions on the FP64
- * tensor cores (DMMA) for NN = 9..19 (other grids always use the FMA
- * kernels).  Both give the reference's H x to rounding. */
-enum { DE_MATVEC_FMA = 0, DE_MATVEC_TENSOR = 1 };
+ * CUDA-core kernels on even/odd-split contractions for NN = 9..21,
+ * DE_MATVEC_TENSOR the axis contractions on the FP64 tensor cores (DMMA)
+ * for NN = 9..19, DE_MATVEC_STREAM the earlier CUDA-core streaming kernels
+ * for NN = 13..19 (kept for comparison).  Other grids use the shared-memory
+ * cube kernels whatever the choice.  All give the reference's H x to
+ * rounding. */
+enum { DE_MATVEC_FMA = 0, DE_MATVEC_TENSOR = 1, DE_MATVEC_STREAM = 2 };
 DE_API int de_set_matvec_kernel(de_problem *h, int kind);
 /* Device milliseconds of pass A and pass B, MATBLOCK calls and vectors
  * multiplied since the last read (waits for the recorded events); resets. */
@@ -190,19 +193,22 @@ DE_API int de_dots_d(de_problem *h, const de_complex *bras_d, const de_complex *
                      int64_t size, int nbra, int nket, de_complex *out_host, int hermitian);
 
 /* Allocation-free device dot products.  No counterpart in the reference.
- * For callers that cannot allocate device memory: code recording work into a
- * CUDA graph, or running inside a pre-reserved memory budget, where a
- * cudaMalloc would break the capture or the reservation.  Same results as
- * de_dots_d (hermitian=1: conj(BRA).KET; 0: the c-product), written to DEVICE
- * memory out_d (nbra x nket column-major) asynchronously on cuda_stream (NULL:
- * legacy default stream).  Needs no handle and allocates nothing: the
- * reduction scratch is a static device array of 151,568 bytes that every GPU
- * loading the library holds until exit.  Shapes: nket == 1 with nbra <= 32,
- * or nbra, nket <= 8 with one of them <= 4 (at most 32 outputs); larger shapes
- * return DE_E_INVALID.  The first call on each device looks up the array's
- * device address (make it before any stream capture).  All calls share the
- * array: calls that overlap on the GPU (other streams, other host threads)
- * race and must be serialised by the caller. */
+ * For callers that cannot call cudaMalloc: code embedded in a host
+ * application that owns all device memory through its own pool or a fixed
+ * reservation (a serving process that reserved its HBM up front), where an
+ * allocation by this library would fail or exceed the reservation.  Same
+ * results as de_dots_d (hermitian=1: conj(BRA).KET; 0: the c-product),
+ * written to DEVICE memory out_d (nbra x nket column-major) asynchronously on
+ * cuda_stream (NULL: legacy default stream).  Needs no handle and calls no
+ * allocating routine: the reduction scratch is a static device array of
+ * 151,568 bytes that every GPU loading the library holds until exit.
+ * Shapes: nket == 1 with nbra <= 32, or nbra, nket <= 8 with one of them <= 4
+ * (at most 32 outputs); larger shapes return DE_E_INVALID.  The first call on
+ * each device (and the first after a device reset) looks up the array's
+ * device address; make that call before any stream capture.  All calls share
+ * the array and each clears its reduction ticket first: calls that overlap
+ * on the GPU (other streams, other host threads) race and must be serialised
+ * by the caller. */
 DE_API int de_dots_noalloc_d(const de_complex *bras_d, const de_complex *kets_d, int64_t size, int nbra,
                              int nket, de_complex *out_d, int hermitian, void *cuda_stream);
 

@@ -1,10 +1,12 @@
 """The allocation-free dot products (de_dots_noalloc_d), for callers that
-cannot allocate device memory (graph recording, fixed memory budgets).
+cannot call cudaMalloc (a host application that owns all device memory
+through its own pool or a fixed reservation).
 
-Checked through the C ABI against the allocating entry point de_dots_d on
-the same device inputs, twice in a row (the calls share one static scratch
-array, so the second call also checks that the first left it reusable).
-Same tolerance as the other dot-product checks here: 1e-12 relative."""
+Checked through the C ABI against the allocating entry point de_dots_d and
+against numpy's products of the same host blocks, twice in a row (the calls
+share one static scratch array, so the second call also checks that the
+first left it reusable).  Same tolerance as the other dot-product checks
+here: 1e-12 relative."""
 import ctypes
 
 import numpy as np
@@ -28,6 +30,7 @@ def test_noalloc_dots_match_allocating_dots(de, nbra, nket, herm):
     a = rng.standard_normal((size, nbra)) + 1j * rng.standard_normal((size, nbra))
     b = rng.standard_normal((size, nket)) + 1j * rng.standard_normal((size, nket))
     ad, bd = _dev(torch, a), _dev(torch, b)
+    want = (a.conj().T if herm else a.T) @ b  # numpy, independent of the library's kernels
     ref = np.empty((nbra, nket), np.complex128, order="F")
     with de.Problem(n=1, delta=2.0, theta=0.3) as g:
         torch.cuda.synchronize()
@@ -43,6 +46,7 @@ def test_noalloc_dots_match_allocating_dots(de, nbra, nket, herm):
         assert s == de.DE_OK, L.de_last_error()
         got = out.cpu().numpy().T
         assert np.linalg.norm(got - ref) <= TOL * np.linalg.norm(ref)
+        assert np.linalg.norm(got - want) <= TOL * np.linalg.norm(want)
 
 
 def test_noalloc_dots_reject_shapes_beyond_the_scratch(de):
