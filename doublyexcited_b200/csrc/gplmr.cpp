@@ -752,6 +752,27 @@ struct Solver {
         return gmres_run(o, gm.max_inner_iter, gm.tol, kGmresRestart, &its);
     }
 
+    // Column equilibration of a block before the BASIC inner solve.  The
+    // blocks GPLMR preconditions are residuals (gplmr.F90:95-101,112-123,
+    // 141-148); once some columns converge their norms differ from the rest
+    // by many orders of magnitude, and the k x k Gram of (H - sigma) V that
+    // harm_orthog_oneblock orthonormalises (harmonic_ritz_small.F90:187-242)
+    // inherits the squared ratio as its condition number: at NEV = 4 the
+    // reference's own 1e-10 self-check then fails ("AACK DOTS") once a column
+    // converges.  The inner solve returns the minimal-residual approximation
+    // of (H - sigma)^-1 B over the block Krylov space of B, which column
+    // scaling leaves unchanged, so its output for B D is its output for B
+    // times D; GPLMR then orthonormalises the block by CholQR, which removes
+    // D.  Scaling every column to unit norm is therefore exact in exact
+    // arithmetic and keeps the Gram's conditioning to that of the column
+    // directions.  One column needs no scaling; the first-column-only mode
+    // keeps the reference's unscaled blocks.
+    int equilibrate(double2 *b, int k)
+    {
+        if (k < 2 || compat) return DE_OK;
+        return normalize(b, k);
+    }
+
     // PRECBLOCK gplmr.F90:466-502 (in place)
     int precblock(double2 *b, int k)
     {
@@ -767,7 +788,8 @@ struct Solver {
             s = DE_OK;
             for (int j = 0; s == DE_OK && j < k; ++j) s = gmres_col(col(b, j));
         } else if (mixed) {
-            s = basic<float2>(b, k);
+            s = equilibrate(b, k);
+            if (s == DE_OK) s = basic<float2>(b, k);
             // FP32 rounding in the inner solve breaks the electron-exchange
             // symmetry that H and the FP64 iteration keep exactly; the
             // contamination would stall the residual near 1e-6.  Restore it.
@@ -776,7 +798,17 @@ struct Solver {
                 if (e != cudaSuccess) s = cuda_error(e, "exch_project");
             }
         } else {
-            s = basic<double2>(b, k);
+            s = equilibrate(b, k);
+            if (s == DE_OK) s = basic<double2>(b, k);
+            // Block solves (NEV > 1) keep the start block's exchange sector
+            // too: in exact arithmetic the iteration never leaves it, but
+            // FP64 rounding leaks into the other sector, and GPLMR then
+            // converges to whichever sector's states lie nearest sigma (at
+            // N = 3, 4 with NEV = 4 a singlet start found a triplet triple).
+            for (int j = 0; s == DE_OK && k > 1 && exch_sign != 0.0 && j < k; ++j) {
+                cudaError_t e = exch_project_launch(col(b, j), h->m, exch_sign, st);
+                if (e != cudaSuccess) s = cuda_error(e, "exch_project");
+            }
         }
         t_prec += secs(t0, clk::now());
         return s;
@@ -811,7 +843,8 @@ struct Solver {
         X = x_dev;
         DE_TRY(setup());
         DE_TRY(normalize(X, nev));
-        if (mixed && order > 1) DE_TRY(detect_exchange_symmetry());
+        if ((mixed || (nev > 1 && !compat)) && order > 1 && gm.usepetscflag != 0)
+            DE_TRY(detect_exchange_symmetry());
         DE_TRY(matblock(X, AX, nev));
         std::vector<cplx> E;
         std::vector<double> res;

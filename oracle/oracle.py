@@ -497,12 +497,32 @@ def petsc_gmres(apply, b: np.ndarray, max_it: int, rtol: float, abstol: float = 
 def gplmr_eig(h: Hamiltonian, x0: np.ndarray, sigma: complex, ns: int = 5, maxit: int = 100,
               tol: float = 1e-7, order: int = 5, compat_first_column_only: bool = False,
               max_inner_iter: int | None = None, verbose: bool = False, usepetscflag: int = 1,
-              gm_tol: float = 1e-3, gm_shift: complex = 0.0) -> GplmrResult:
+              gm_tol: float = 1e-3, gm_shift: complex = 0.0, equilibrate: bool = True,
+              exchange_project: bool = True) -> GplmrResult:
     """GPLMR_EIG gplmr.F90:9-374 with the BASIC preconditioner, or with
     usepetscflag = 0 the PETSc GMRES one (PRECBLOCK gplmr.F90:466-502):
     GMRES on (H - gm_shift) per column with rtol gm_tol.  The reference's
     GMSOLVER%SHIFT is never assigned and lives in the main program's
-    zero-initialised storage, so gm_shift defaults to 0."""
+    zero-initialised storage, so gm_shift defaults to 0.
+
+    equilibrate (default on; off restates the reference exactly): with
+    NEV > 1 the residual block handed to PRECBLOCK_BASIC is scaled to unit
+    columns first.  The reference passes the raw residuals
+    (gplmr.F90:95-101); once a column converges, the Gram of (H - sigma) V
+    in harm_orthog_oneblock (harmonic_ritz_small.F90:187-242) has a
+    condition number near the squared ratio of the column norms (4e10 at
+    N=3, NEV=4, iteration 21) and the 1e-10 self-check stops the run.  The
+    inner solve's output is linear in column scaling (a minimal-residual
+    solve over the block Krylov space, which scaling leaves unchanged) and
+    GPLMR's next step, cholQR, removes the scale, so the iteration is the
+    same in exact arithmetic.  The first-column-only mode is never scaled.
+
+    exchange_project (default on; off restates the reference): a block
+    solve (NEV > 1, BASIC path) whose start columns are all exchange-
+    symmetric (or all antisymmetric) projects each preconditioned block back
+    onto that sector, X <- (X +- X^T)/2.  Exact arithmetic never leaves the
+    sector; rounding does, and at N = 3, 4 with NEV = 4 a singlet start
+    otherwise converges to a triplet triple nearer sigma."""
     if max_inner_iter is None:
         max_inner_iter = order
     calls0 = h.calls
@@ -528,9 +548,31 @@ def gplmr_eig(h: Hamiltonian, x0: np.ndarray, sigma: complex, ns: int = 5, maxit
                 return out
             return h.matblock(v)
 
-        return basicblocklansolve(blk, max_inner_iter, h.params.m ** 2, sigma, mult)
+        if equilibrate and not compat_first_column_only and blk.shape[1] > 1:
+            # unit columns: the inner solve's output is linear in column
+            # scaling and cholQR removes it again, so only the conditioning
+            # of harm_orthog_oneblock's Gram changes (see gplmr_eig)
+            blk = blk / colnorms(blk)[None, :]
+        out = basicblocklansolve(blk, max_inner_iter, h.params.m ** 2, sigma, mult)
+        if exch_sign != 0.0 and blk.shape[1] > 1:
+            m = h.params.m
+            for j in range(out.shape[1]):
+                z = out[:, j].reshape(m, m, order="F")
+                out[:, j] = (0.5 * (z + exch_sign * z.T)).reshape(-1, order="F")
+        return out
 
     x /= colnorms(x)[None, :]
+    # exchange sector of the start block (+1 every column symmetric, -1
+    # every column antisymmetric, 0 otherwise), kept by block solves
+    exch_sign = 0.0
+    if exchange_project and nev > 1 and not compat_first_column_only and usepetscflag != 0 and max_inner_iter > 1:
+        m = h.params.m
+        signs = []
+        for j in range(nev):
+            z = x[:, j].reshape(m, m, order="F")
+            r = float(np.vdot(z.reshape(-1), z.T.reshape(-1)).real)
+            signs.append(1.0 if abs(r - 1.0) < 1e-8 else -1.0 if abs(r + 1.0) < 1e-8 else 0.0)
+        exch_sign = signs[0] if all(sg == signs[0] for sg in signs) else 0.0
     ax = h.matblock(x)
     e = np.einsum("ij,ij->j", x.conj(), ax)
     w = ax - x * e[None, :]

@@ -241,6 +241,7 @@ FIXTURES = {
     "hammult1_n5": (False, lambda: ("npz", hammult1_fixture(5, 0.2, 15))),
     "gplmr_n3_nev1": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 1, False, 60, 1e-10))),
     "gplmr_n3_nev4": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 4, False, 12, 1e-10))),
+    "gplmr_n3_nev4_conv": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 4, False, 300, 1e-9))),
     "gplmr_n3_nev4_compat": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 4, True, 12, 1e-10))),
     "gplmr_n3_nev1_petsc": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 1, False, 80, 1e-10,
                                                                  usepetscflag=0))),
