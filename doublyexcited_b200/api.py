@@ -100,11 +100,14 @@ class Problem:
         check(lib().de_set_stream(self._h, ctypes.c_void_p(cuda_stream)), "de_set_stream")
 
     def set_matvec_kernel(self, kind: str) -> None:
-        """'fma' (default): the CUDA-core kernels; 'tensor': the axis
-        contractions on the FP64 tensor cores where built (NN 9..19)."""
-        if kind not in ("tensor", "fma"):
-            raise ValueError("kind must be 'tensor' or 'fma'")
-        check(lib().de_set_matvec_kernel(self._h, 1 if kind == "tensor" else 0), "de_set_matvec_kernel")
+        """'fma' (default): the CUDA-core kernels on even/odd-split
+        contractions; 'tensor': the axis contractions on the FP64 tensor
+        cores where built (NN 9..19); 'stream': the earlier CUDA-core
+        streaming kernels (NN 13..19)."""
+        kinds = {"fma": 0, "tensor": 1, "stream": 2}
+        if kind not in kinds:
+            raise ValueError(f"matvec kernel must be one of {sorted(kinds)}")
+        check(lib().de_set_matvec_kernel(self._h, kinds[kind]), "de_set_matvec_kernel")
 
     def set_profiling(self, on: bool) -> None:
         check(lib().de_set_profiling(self._h, int(bool(on))), "de_set_profiling")

@@ -315,7 +315,7 @@ DE_API int de_problem_create(const de_params *pin, de_problem **out)
     hd.vsim = vs.imag();
     hd.sre = scale.real();
     hd.sim = scale.imag();
-    hd.tc = 0;  // the CUDA-core kernels are faster on B200 so far (de_set_matvec_kernel)
+    hd.tc = 0;  // the even/odd CUDA-core kernels (de_set_matvec_kernel)
 
     auto tinv = cached_tinv(nbig_alloc, nbig_solve, p.nsmall, delta);
     const int nbd = 2 * nbig_alloc + 1;
@@ -334,6 +334,7 @@ DE_API int de_problem_create(const de_params *pin, de_problem **out)
     hd.v12 = h->d_v12;
     // FP32 copies of T and of the potential tables for the mixed form
     for (int d = 0; d < nn; ++d) hd.tf[d] = (float)t[d];
+    fill_ev_coefficients(hd);
     DE_CUDA(cudaMallocAsync(&h->d_t1af, h->m * sizeof(float), h->stream));
     DE_CUDA(cudaMallocAsync(&h->d_v12f, w * w * w * sizeof(float), h->stream));
     ce = to_f32_launch(h->d_t1a, h->d_t1af, h->m, h->stream);
@@ -399,10 +400,11 @@ DE_API int de_set_stream(de_problem *h, void *s)
 DE_API int de_set_matvec_kernel(de_problem *h, int kind)
 {
     if (!h) return set_error(DE_E_INVALID, "null handle");
-    if (kind != DE_MATVEC_FMA && kind != DE_MATVEC_TENSOR)
-        return set_error(DE_E_INVALID, "matvec kernel must be DE_MATVEC_FMA or DE_MATVEC_TENSOR (got %d)", kind);
+    if (kind != DE_MATVEC_FMA && kind != DE_MATVEC_TENSOR && kind != DE_MATVEC_STREAM)
+        return set_error(DE_E_INVALID,
+                         "matvec kernel must be DE_MATVEC_FMA, DE_MATVEC_TENSOR or DE_MATVEC_STREAM (got %d)", kind);
     std::lock_guard<std::mutex> lk(h->mu);
-    h->ham.tc = kind == DE_MATVEC_TENSOR;
+    h->ham.tc = kind;
     return DE_OK;
 }
 

@@ -13,6 +13,7 @@ void count_launch(int n = 1);
 int64_t launch_count();
 
 constexpr int kMaxNN = 27;      // N <= 13 (the reference ran N = 5..15)
+constexpr int kEvCoef = 12 * 12;  // even/odd coefficient tables, N <= 11
 constexpr int kMaxCols = 128;   // columns per block-op operand list
 
 // Operator data for one problem (HAMILTONIAN, structs.F90:87-102).
@@ -30,8 +31,17 @@ struct HamDev {
     float tf[kMaxNN];
     const float *t1af;
     const float *v12f;
-    int tc;  // 1: axis contractions on the FP64 tensor cores where built (hammult_tc.cu)
+    int tc;  // matvec kernels: 0 even/odd (hammult_ev.cu), 1 FP64 tensor cores (hammult_tc.cu),
+             // 2 the earlier streaming kernels (hammult.cu)
+    // Even/odd-split coefficients of T for the grid (hammult_ev.cu), index
+    // a * (N+1) + b: ev_ce(a,0) = t(a), ev_ce(a,b) = (t(|a-b|) + t(a+b))/2,
+    // ev_co(a,b) = (t(|a-b|) - t(a+b))/2 (a, b >= 1); FP32 copies beside.
+    double ev_ce[kEvCoef], ev_co[kEvCoef];
+    float ev_cef[kEvCoef], ev_cof[kEvCoef];
 };
+
+// Fills ev_ce / ev_co (and the FP32 copies) from h.t for grid h.nn.
+void fill_ev_coefficients(HamDev &h);
 
 // Y(:,:,v) = H X(:,:,v) for v < nvec; vectors are vstride elements apart.
 // Two passes: electron-2 axes + potential (strided cubes, writes Y), then
@@ -47,6 +57,15 @@ cudaError_t hammult_pass_launch(const HamDev &h, const double2 *x, double2 *y, i
 // The same on complex64 vectors in FP32 arithmetic (needs h.tf / t1af / v12f).
 cudaError_t hammult_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride, int pass,
                                 cudaStream_t st, double2 shift = double2{0.0, 0.0});
+
+// Even/odd-split form of one pass (hammult_ev.cu) for the grids
+// hammult_ev_supported accepts (complex128: NN = 9..15; complex64: NN =
+// 9..21); shs is the diagonal shift times SCALE^2.
+bool hammult_ev_supported(int nn, bool fp64);
+cudaError_t hammult_ev_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,
+                                   int pass, cudaStream_t st, double2 shs);
+cudaError_t hammult_ev_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride, int pass,
+                                   cudaStream_t st, double2 shs);
 
 // Tensor-core (DMMA) form of one pass, for the grids hammult_tc_supported
 // accepts; the same arguments and results as hammult_pass_launch.

@@ -34,6 +34,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 
 namespace de {
 namespace {
@@ -625,6 +626,24 @@ cudaError_t dispatch(const HamDev &h, const CubeArgs<R> &a, int64_t ncubes, cuda
 
 }  // namespace
 
+void fill_ev_coefficients(HamDev &h)
+{
+    const int nn = h.nn, n = nn / 2;
+    for (int i = 0; i < kEvCoef; ++i) h.ev_ce[i] = h.ev_co[i] = 0.0;
+    if (n + 1 > 12) return;
+    auto t = [&](int d) { return d < nn ? h.t[d] : 0.0; };
+    for (int a = 0; a <= n; ++a)
+        for (int b = 0; b <= n; ++b) {
+            const int idx = a * (n + 1) + b;
+            h.ev_ce[idx] = b == 0 ? t(a) : 0.5 * (t(std::abs(a - b)) + t(a + b));
+            h.ev_co[idx] = (a >= 1 && b >= 1) ? 0.5 * (t(std::abs(a - b)) - t(a + b)) : 0.0;
+        }
+    for (int i = 0; i < kEvCoef; ++i) {
+        h.ev_cef[i] = (float)h.ev_ce[i];
+        h.ev_cof[i] = (float)h.ev_co[i];
+    }
+}
+
 template <class R>
 static CubeArgs<R> make_args(const HamDev &h, const C2<R> *x, C2<R> *y, int64_t vstride, double2 shift)
 {
@@ -641,8 +660,13 @@ static cudaError_t pass_go(const HamDev &h, const C2<R> *x, C2<R> *y, int nvec, 
 {
     if (h.nelec != 2 || nvec <= 0) return cudaErrorInvalidValue;
     if (sizeof(R) == 4 && (!h.t1af || !h.v12f)) return cudaErrorInvalidValue;
-    if (h.tc && hammult_tc_supported(h.nn)) return hammult_tc_pass_launch(h, x, y, nvec, vstride, pass, st, shift);
+    if (h.tc == 1 && hammult_tc_supported(h.nn)) return hammult_tc_pass_launch(h, x, y, nvec, vstride, pass, st, shift);
     const CubeArgs<R> a = make_args<R>(h, x, y, vstride, shift);
+    // even/odd kernels where built: complex128 up to NN = 15 (above it their
+    // k-line accumulators exceed the registers a thread has and the
+    // streaming kernels are faster), complex64 up to NN = 21
+    if (h.tc == 0 && hammult_ev_supported(h.nn, sizeof(R) == 8))
+        return hammult_ev_pass_launch(h, x, y, nvec, vstride, pass, st, a.shs);
     const int64_t ncubes = h.m * (int64_t)nvec;
     if (ncubes > 0x7fffffffLL) return cudaErrorInvalidValue;
     return pass == 0 ? dispatch<R, kRowsPot>(h, a, ncubes, st) : dispatch<R, kColsAcc>(h, a, ncubes, st);
