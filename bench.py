@@ -158,10 +158,22 @@ def alg_bytes(nn):
     return 32 * nn ** 6
 
 
-# dram bytes (read + write) per vector-matvec (pass A + pass B), keyed by
-# (NN, storage), from the ncu capture of the block-of-2 matvec at N=6
-# (profiles/stream_kernel_matvec-n6.md): both passes' bytes over 2 vectors.
-NCU_TRAFFIC_PER_VECTOR = {(13, "f64"): 342.25e6, (13, "f32"): 151.8e6}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, pass A + pass B)
+# per vector-matvec of the default (even/odd) kernels, keyed by (NN,
+# storage): one ncu capture of a block-of-2 matvec per grid (the
+# `--workload matvec-n*` small cases), both passes' bytes over 2 vectors.
+# Grids without a capture report null.
+NCU_TRAFFIC_PER_VECTOR = {}
+
+
+def solve_config(a, w):
+    """The workload's config dict, printed identically by both arms."""
+    nn = 2 * w["n"] + 1
+    return {"workload": a.workload, "start": a.start, "N": w["n"], "NN": nn, "dim": nn ** 6, "nev": w["nev"],
+            "ns": w["ns"], "order": w["order"], "theta": w["theta"], "delta": w["delta"], "sigma": w["sigma"],
+            "tol": w["tol"], "spin": w["spin"], "seed": w["seed"],
+            "l2": "inputs larger than L2 (GPLMR workspace "
+                  f"{(17 + 2 * w['order']) * w['nev'] * nn ** 6 * 16 / 1e9:.1f} GB per solve)"}
 
 
 class ClockSampler:
@@ -293,35 +305,55 @@ def dist_setup():
     return rank, world, local
 
 
+def oracle_iteration_seconds(w):
+    """Wall seconds of one complete GPLMR iteration of the oracle (the
+    reference's loops restated: C HAMMULT with OpenMP over all host cores,
+    the BASIC inner solve and every block operation in numpy/LAPACK) from
+    the workload's start block: gplmr_eig with maxit=1, which also forms the
+    start block's products and residuals."""
+    from oracle import oracle as O  # the reference arm's CPU restatement
+
+    p = O.Params(n=w["n"], delta=w["delta"], theta=w["theta"])
+    h = O.init_hamiltonian(p, nelec=2)
+    x0 = O.seeded_start(p, w["nev"], w["seed"], w["spin"])
+    t0 = time.perf_counter()
+    O.gplmr_eig(h, x0, complex(w["sigma"], 0.0), ns=w["ns"], maxit=1, tol=0.0, order=w["order"])
+    return time.perf_counter() - t0, os.cpu_count()
+
+
 def run_reference(a, w):
+    """--impl reference: the reference's CPU path (the oracle restatement: the
+    Fortran/MPI/PETSc program cannot be built on this image) on the same
+    workload.  One step = one complete GPLMR iteration, block operations
+    included; ms_per_step is that measured time.  solves/s = 1 / (median
+    step time x the workload's iterations to convergence)."""
     rank, world, local = dist_setup()
     if rank != 0:
         return 0
     iters = w["iters_ref"]
     if iters is None:
-        print(json.dumps({"impl": "reference", "unavailable": "no converged iteration count recorded for this workload"}))
+        print(json.dumps({"impl": "reference", "unavailable": "no converged iteration count recorded for this "
+                                                              "workload (a complete CPU solve takes hours)"}))
         return 0
-    nmv = hammults_per_solve(w, iters)
     for _ in range(a.warmup):
-        cpu_matvec_seconds(w, 1)
+        oracle_iteration_seconds(w)
     times = []
+    cores = os.cpu_count()
     for _ in range(a.steps):
-        t, cores = cpu_matvec_seconds(w, 2)
+        t, cores = oracle_iteration_seconds(w)
         times.append(t)
-    t_mv = statistics.median(times)
-    solve_s = nmv * t_mv
-    v = 1.0 / solve_s
-    nn = 2 * w["n"] + 1
+    t_it = statistics.median(times)
+    v = 1.0 / (t_it * iters)
     line = {
         "impl": "reference", "metric": "resonance solves/s", "value": v, "unit": "solves/s", "n_gpus": a.gpus,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": solve_s * 1e3, "higher_is_better": True,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_it * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": a.workload, "N": w["n"], "NN": nn, "dim": nn ** 6, "nev": w["nev"], "ns": w["ns"],
-                   "order": w["order"], "theta": w["theta"], "delta": w["delta"], "tol": w["tol"],
-                   "parallelism": "cpu-openmp"},
+        "config": solve_config(a, w),
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                         "sample": f"{2 * a.steps} oracle HAMMULTs at N={w['n']} (C, OpenMP, all cores), "
-                                   f"x {nmv} HAMMULTs per solve ({iters} GPLMR iterations); block ops not charged"},
+                         "sample": f"one step = one complete GPLMR iteration of the oracle at N={w['n']} (C HAMMULT "
+                                   f"with OpenMP on {cores} threads, BASIC inner solve and block operations in "
+                                   f"numpy/LAPACK); solves/s = 1 / (median {t_it:.2f} s x {iters} iterations "
+                                   f"to converge)"},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -653,10 +685,12 @@ def main():
     x_work = torch.empty_like(x_pin).pin_memory()
     xw = x_work.numpy().view(np.complex128).reshape(x0.shape, order="F")
     prob.set_stream(0)
+    # the same K steps and the same profiling state as the device-timed value
+    prob.set_profiling(True)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
-    e2e_steps = max(1, min(a.steps, 2))
+    e2e_steps = a.steps
     for _ in range(e2e_steps):
         np.copyto(xw, x_host)
         st2 = de_stats()
@@ -665,6 +699,9 @@ def main():
                              ctypes.byref(st2)), "de_gplmr_eig")
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
+    prob.profile_read()
+    prob.profile_read32()
+    prob.set_profiling(False)
     if pg:
         t_e2e = max_over_ranks(t_e2e, pg, "cuda")
     e2e = replica_rate(e2e_steps, world, t_e2e)
@@ -698,12 +735,12 @@ def main():
         roofline, roofline_other = roof64, roof32
 
     cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        t_mv, cores = cpu_matvec_seconds(w, 3)
-        nmv = st.matvecs_reference
-        cpu = {"value": 1.0 / (nmv * t_mv), "unit": "solves/s", "cores": cores, "kind": "port",
-               "sample": f"3 oracle HAMMULTs at N={w['n']} (C, OpenMP over columns, {cores} threads) "
-                         f"= {t_mv:.3f} s each, x {nmv} HAMMULTs per solve; block ops not charged"}
+    if rank == 0 and world == 1 and not a.no_cpu_baseline and w["n"] <= 6:
+        t_it, cores = oracle_iteration_seconds(w)
+        cpu = {"value": 1.0 / (t_it * st.iterations), "unit": "solves/s", "cores": cores, "kind": "port",
+               "sample": f"one complete GPLMR iteration of the oracle at N={w['n']} ({t_it:.2f} s: C HAMMULT with "
+                         f"OpenMP on {cores} threads, BASIC inner solve and block operations in numpy/LAPACK) "
+                         f"x the {st.iterations} iterations this solve took"}
 
     compare = {"fp64_error": other_err} if other_err else None
     if other is not None:
@@ -724,13 +761,8 @@ def main():
             "data": ("synthetic (seeded complex-Gaussian singlet start vector; operator from the reference's physics)"
                      if a.start == "seeded" else
                      "synthetic operator from the reference's physics; start block from the reference's initial guess"),
-            "config": {"workload": a.workload, "start": a.start,
-                       "N": w["n"], "NN": nn, "dim": dim, "nev": w["nev"], "ns": w["ns"],
-                       "order": w["order"], "theta": w["theta"], "delta": w["delta"], "sigma": w["sigma"],
-                       "tol": w["tol"], "precision": a.precision,
-                       "l2": "inputs larger than L2 (GPLMR workspace "
-                             f"{(17 + 2 * w['order']) * w['nev'] * dim * 16 / 1e9:.1f} GB per solve)",
-                       "parallelism": f"replicas x{world}"},
+            "config": solve_config(a, w),
+            "precision": a.precision, "parallelism": f"replicas x{world}",
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": int(x0.nbytes),
                     "d2h_bytes_per_step": int(x0.nbytes + e_host.nbytes)},
             "roofline": roofline,
