@@ -69,7 +69,8 @@ struct Solver {
     // iterate and the residual; small device scalars
     static constexpr int kGmresRestart = 30;
     double2 *GV = nullptr, *dGs = nullptr;
-    float2 *LV32 = nullptr, *LQ32 = nullptr;  // the same in complex64 (mixed)
+    float2 *LV32 = nullptr, *LQ32 = nullptr;  // the same in complex64 (unused by the mixed s-step solve)
+    float2 *Z32 = nullptr;  // mixed inner solve: the power basis Z_0..Z_order (complex64)
     bool mixed = false;
     double exch_sign = 0.0;  // +1 / -1: exchange symmetry of the start block (mixed form), 0: none
     // The mixed form's self-check: complex64 rounding amplified by the
@@ -79,6 +80,13 @@ struct Solver {
     double2 *dRinv = nullptr, *dGinvh = nullptr, *dGsq = nullptr, *dG1 = nullptr, *dSV = nullptr;
     int *dFlags = nullptr;
     double2 *hbuf = nullptr;  // pinned staging for k x k results (>= 64 x 128 + 64)
+    // Uploads of small coefficient matrices go through a ring of pinned slots
+    // above the download area, each guarded by an event, so that an upload
+    // never waits for the stream (it waits only if its slot's previous copy
+    // is still in flight, four uploads later).
+    static constexpr int kUpSlots = 4, kUpSlotElems = 1920, kUpBase = 64 * 136;
+    cudaEvent_t up_ev[kUpSlots] = {};
+    int up_next = 0;
     std::vector<double2 *> allocs;
 
     int64_t mv_exec = 0, mv_ref = 0;
@@ -87,6 +95,8 @@ struct Solver {
     ~Solver()
     {
         for (auto p : allocs) h->cache_put(p);
+        for (cudaEvent_t e : up_ev)
+            if (e) cudaEventDestroy(e);
     }
 
     double2 *col(double2 *b, int j) const { return b + (int64_t)j * D; }
@@ -115,9 +125,9 @@ struct Solver {
             DE_TRY(alloc(&dGs, 128));
         } else if (order > 0) {
             const int64_t n = D * (int64_t)std::max(1, order) * nev;
-            if (mixed && order > 1) {  // complex64: half the bytes
-                DE_TRY(alloc(reinterpret_cast<double2 **>(&LV32), (n + 1) / 2));
-                DE_TRY(alloc(reinterpret_cast<double2 **>(&LQ32), (n + 1) / 2));
+            if (mixed && order > 1) {  // complex64 power basis, (order + 1) blocks
+                const int64_t nz = D * (int64_t)(order + 1) * nev;
+                DE_TRY(alloc(reinterpret_cast<double2 **>(&Z32), (nz + 1) / 2));
             } else {
                 DE_TRY(alloc(&LV, n));
                 DE_TRY(alloc(&LQ, n));
@@ -141,6 +151,7 @@ struct Solver {
             DE_CUDA(cudaMemsetAsync(dFlags, 0, 4 * sizeof(double2), st));
         }
         hbuf = h->h_small;  // pinned, 64 x 256 (the handle is locked for the solve)
+        for (cudaEvent_t &e : up_ev) DE_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         const int64_t wk = std::max<int64_t>(gram_work_elems(64, 128, D), dotdiag_work_elems(64, D));
         DE_TRY(h->ensure_work(wk));
         return DE_OK;
@@ -220,9 +231,14 @@ struct Solver {
 
     int upload(const std::vector<cplx> &m, double2 *dst)
     {
-        for (size_t i = 0; i < m.size(); ++i) hbuf[i] = make_double2(m[i].real(), m[i].imag());
-        DE_CUDA(cudaMemcpyAsync(dst, hbuf, m.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
-        DE_CUDA(cudaStreamSynchronize(st));  // hbuf is reused
+        if (m.size() > (size_t)kUpSlotElems) return set_error(DE_E_INVALID, "coefficient upload too large");
+        const int slot = up_next;
+        up_next = (up_next + 1) % kUpSlots;
+        DE_CUDA(cudaEventSynchronize(up_ev[slot]));  // the slot's previous copy has left
+        double2 *src = hbuf + kUpBase + (size_t)slot * kUpSlotElems;
+        for (size_t i = 0; i < m.size(); ++i) src[i] = make_double2(m[i].real(), m[i].imag());
+        DE_CUDA(cudaMemcpyAsync(dst, src, m.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+        DE_CUDA(cudaEventRecord(up_ev[slot], st));
         return DE_OK;
     }
 
@@ -773,6 +789,75 @@ struct Solver {
         return normalize(b, k);
     }
 
+    // The mixed form's inner solve.  The same minimal-residual approximation
+    // of (H - sigma)^-1 B over the block Krylov space K_order(H, B) that
+    // basicblocklansolve forms (harmonic_ritz_small.F90:258-324: its output
+    // is V Q^H B with Q = (H - sigma) V orthonormal), computed from the power
+    // basis Z_0 = B, Z_i = (H - sigma) Z_{i-1} instead of a Gram-Schmidt
+    // basis: with Q = [Z_1 .. Z_order] = (H - sigma) [Z_0 .. Z_order-1] the
+    // solution is Y = [Z_0 .. Z_order-1] a with (Q^H Q) a = Q^H B, so one Gram
+    // of the Z blocks (FP64 sums over complex64 vectors) and one update
+    // replace the Gram-Schmidt passes: about 20 vector passes per call
+    // instead of about 120 at NEV = 1.  The normal equations are solved on
+    // the host after diagonal scaling through an SVD that drops singular
+    // values below 1e-13 of the largest (the basis is far from orthogonal;
+    // this is a preconditioner, and the FP64 outer iteration refines every
+    // Ritz pair).
+    int basic_sstep(double2 *b, int k)
+    {
+        const int nq = order * k, nz = (order + 1) * k;
+        {
+            cudaError_t e = to_f32_launch(b, Z32, (int64_t)k * D, st);
+            if (e != cudaSuccess) return cuda_error(e, "to_f32");
+        }
+        for (int i = 1; i <= order; ++i)
+            DE_TRY(mult_shifted<float2>(Z32 + (int64_t)(i - 1) * k * D, Z32 + (int64_t)i * k * D, k));
+        mv_ref += (order + 1) * k;  // the reference forms (2 order + 1) k products
+        std::vector<cplx> g;  // [Z_1..Z_order]^H [Z_0..Z_order], nq x nz
+        DE_TRY(gram_hostT(colsT(Z32 + (int64_t)k * D, nq, D), colsT(Z32, nz, D), g));
+        auto t0 = clk::now();
+        std::vector<cplx> a;
+        DE_TRY(minres_normal(nq, k, g, a));
+        t_dense += secs(t0, clk::now());
+        DE_TRY(upload(a, dC));
+        return updateT(Z32, nq, b, k, dC, nq);
+    }
+
+    // Solves (Q^H Q) a = Q^H B from g = Q^H [B Q] (nq x (k + nq)): diagonal
+    // scaling, then the pseudo-inverse of the scaled Gram from zgesdd.
+    int minres_normal(int nq, int k, const std::vector<cplx> &g, std::vector<cplx> &a)
+    {
+        const Lapack &L = lapack();
+        std::vector<double> d(nq);
+        for (int i = 0; i < nq; ++i) {
+            const double v = g[i + (size_t)nq * (k + i)].real();
+            if (!(v > 0.0) || !std::isfinite(v)) return set_error(DE_E_NAN, "inner-solve basis vector %d is zero", i);
+            d[i] = std::sqrt(v);
+        }
+        std::vector<cplx> gs((size_t)nq * nq), u((size_t)nq * nq), vt((size_t)nq * nq);
+        for (int j = 0; j < nq; ++j)
+            for (int i = 0; i < nq; ++i) gs[i + (size_t)nq * j] = g[i + (size_t)nq * (k + j)] / (d[i] * d[j]);
+        std::vector<double> sv(nq), rwork(20 * nq * nq + 100);
+        std::vector<cplx> zwork(20 * nq * nq + 100);
+        std::vector<int> iwork(100 * nq);
+        const int lwork = (int)zwork.size();
+        int info = 0;
+        L.zgesdd("A", &nq, &nq, gs.data(), &nq, sv.data(), u.data(), &nq, vt.data(), &nq, zwork.data(), &lwork,
+                 rwork.data(), iwork.data(), &info, 1);
+        if (info != 0) return set_error(DE_E_SVD, "zgesdd info=%d", info);
+        a.assign((size_t)nq * k, 0.0);
+        for (int l = 0; l < nq; ++l) {
+            if (!(sv[l] > 1e-13 * sv[0])) continue;
+            for (int j = 0; j < k; ++j) {
+                cplx t = 0.0;  // (u_l^H rhs_j) / s_l, rhs scaled by 1/d
+                for (int i = 0; i < nq; ++i) t += std::conj(u[i + (size_t)nq * l]) * g[i + (size_t)nq * j] / d[i];
+                t /= sv[l];
+                for (int i = 0; i < nq; ++i) a[i + (size_t)nq * j] += std::conj(vt[l + (size_t)nq * i]) * t / d[i];
+            }
+        }
+        return DE_OK;
+    }
+
     // PRECBLOCK gplmr.F90:466-502 (in place)
     int precblock(double2 *b, int k)
     {
@@ -789,7 +874,7 @@ struct Solver {
             for (int j = 0; s == DE_OK && j < k; ++j) s = gmres_col(col(b, j));
         } else if (mixed) {
             s = equilibrate(b, k);
-            if (s == DE_OK) s = basic<float2>(b, k);
+            if (s == DE_OK) s = basic_sstep(b, k);
             // FP32 rounding in the inner solve breaks the electron-exchange
             // symmetry that H and the FP64 iteration keep exactly; the
             // contamination would stall the residual near 1e-6.  Restore it.
