@@ -369,6 +369,31 @@ def basicblocklansolve(x: np.ndarray, order: int, maxiter: int, sigma: complex, 
     return vf[:, :thisdim] @ solve
 
 
+def sstep_minres(x: np.ndarray, order: int, sigma: complex, mult, store=None) -> np.ndarray:
+    """The library's mixed-form inner solve: the same minimal-residual
+    approximation of (H - sigma)^{-1} X over the block Krylov space
+    K_order(H, X) as basicblocklansolve, from the power basis Z_0 = X,
+    Z_i = (H - sigma) Z_{i-1} and one Gram: with Q = [Z_1..Z_order] the
+    solution is [Z_0..Z_order-1] a, (Q^H Q) a = Q^H X, solved after diagonal
+    scaling through an SVD that drops singular values below 1e-13 of the
+    largest.  `store` rounds every basis block as the library stores it
+    (complex64 in the mixed form)."""
+    k = x.shape[1]
+    rnd = store if store is not None else (lambda v: v)
+    z = [rnd(x)]
+    for _ in range(order):
+        z.append(rnd(mult(z[-1]) - sigma * z[-1]))
+    zf = np.concatenate(z, axis=1)
+    q = zf[:, k:]
+    g = q.conj().T @ zf
+    gq, rhs = g[:, k:], g[:, :k]
+    d = np.sqrt(np.real(np.diag(gq)))
+    u, sv, vh = np.linalg.svd(gq / d[:, None] / d[None, :])
+    keep = sv > 1e-13 * sv[0]
+    a = (vh[keep].conj().T / sv[keep]) @ (u[:, keep].conj().T @ (rhs / d[:, None]))
+    return zf[:, :order * k] @ (a / d[:, None])
+
+
 # --------------------------------------------------------------------------
 # GPLMR (gplmr.F90)
 

@@ -275,3 +275,22 @@ def test_order20_basic_run_reproduces_the_reference_n6_log():
     assert 0.5 < g["history"][-1]["res"][0] / ref["err"] < 2.0
     assert abs(complex(*g["e"][0]) - complex(*ref["e"])) < 1e-9
     assert g["matvecs_gplmr"] == 1 + g["iterations"] * 6 * 42
+
+
+def test_power_basis_inner_solve_equals_basicblocklansolve():
+    """The mixed form's inner solve (power basis, one Gram) and the
+    reference's basicblocklansolve (Gram-Schmidt basis) compute the same
+    minimal-residual approximation of (H - sigma)^-1 X over the same block
+    Krylov space: in FP64 they agree to the conditioning of the power basis,
+    for one column and for a block of three."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    p = O.Params(n=2, delta=2.0, theta=0.3)
+    h = O.init_hamiltonian(p, nelec=2)
+    for k in (1, 3):
+        x = O.seeded_start(p, k, 7)
+        ref = O.basicblocklansolve(x, 5, p.m ** 2, complex(-0.78, 0.0), h.matblock)
+        got = O.sstep_minres(x, 5, complex(-0.78, 0.0), h.matblock)
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-8
