@@ -91,7 +91,7 @@ def serve_requests(cfg):
     t = 0.0
     out = []
     for k in range(cfg["requests"]):
-        t += rng.exponential(1.0 / cfg["rate"])
+        t += rng.exponential(1.0 / cfg["rate"]) if cfg["rate"] else 0.0
         out.append(dict(t=t, n=int(rng.choice(cfg["ns"], p=cfg["n_weights"])), theta=float(rng.choice(cfg["thetas"])),
                         nev=int(rng.choice(cfg["nevs"])), spin=str(rng.choice(cfg["spins"])), seed=1000 + k))
     return out
@@ -532,6 +532,10 @@ def serve_main(a):
         return 0
     torch.cuda.set_device(local)
     cfg = dict(SERVE)
+    if a.workload == "batch":
+        # the batched configuration restated: 64 uneven problems all queued
+        # at once, from the reference's initial guess, 1, 2 or 4 resonances
+        cfg.update(requests=64, rate=0.0, seed=3, start="guess", nevs=[1, 2, 4])
     if a.workers:
         cfg["workers"] = a.workers
     if a.start == "guess":  # starts from the initial guess: several resonances per request
@@ -552,18 +556,23 @@ def serve_main(a):
     fp64 = run_served(de, seeded_start, cfg, "fp64")
     # the plain FP64 solver: one solve at a time, in arrival order
     plain = run_served(de, seeded_start, cfg, "fp64", workers=1)
+    # the mixed solver one solve at a time (what concurrency adds)
+    mixed1 = run_served(de, seeded_start, cfg, "mixed", workers=1) if a.workload == "batch" else None
     both = [i for i in mixed["e"] if mixed["conv"][i] and fp64["conv"][i]]
     de_max = max((float(np.max(np.abs(np.sort_complex(mixed["e"][i]) - np.sort_complex(fp64["e"][i]))))
                   for i in both), default=None)
     strip = lambda d: {k: v for k, v in d.items() if k not in ("e", "conv")}  # noqa: E731
-    line = {"metric": "resonance solves/s (served stream)", "value": mixed["solves_per_s"], "unit": "solves/s",
+    name = "batched uneven solves" if a.workload == "batch" else "served stream"
+    line = {"metric": f"resonance solves/s ({name})", "value": mixed["solves_per_s"], "unit": "solves/s",
             "n_gpus": 1, "steps": cfg["requests"], "warmup": 2 * len(cfg["ns"]), "ms_per_step": mixed["wall_s"] / cfg["requests"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 inner solve / f64 outer iteration", "data": "synthetic (seeded Poisson arrivals, "
+            "dtype": "f32 inner solve / f64 outer iteration", "data": ("synthetic (64 problems queued at once, " if a.workload == "batch" else
+                                                                   "synthetic (seeded Poisson arrivals, ")
                     + ("starts from the reference's initial guess)" if cfg.get("start") == "guess" else "seeded starts)"),
-            "config": {"workload": "serve", **{k: v for k, v in cfg.items()}},
+            "config": {"workload": a.workload, **{k: v for k, v in cfg.items()}},
             "p50_s": mixed["p50_s"], "p99_s": mixed["p99_s"], "mixed": strip(mixed), "fp64": strip(fp64),
             "fp64_one_at_a_time": strip(plain),
+            "mixed_one_at_a_time": strip(mixed1) if mixed1 else None,
             "speedup_vs_fp64": mixed["solves_per_s"] / fp64["solves_per_s"],
             "speedup_vs_plain_fp64_solver": mixed["solves_per_s"] / plain["solves_per_s"],
             "dE_mixed_vs_fp64_max": de_max,
@@ -579,7 +588,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="solve-n6", choices=sorted(WORKLOADS) + sorted(MATVEC) + ["serve"])
+    ap.add_argument("--workload", default="solve-n6",
+                    choices=sorted(WORKLOADS) + sorted(MATVEC) + ["serve", "batch"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="mixed: FP32 inner solve, FP64 outer iteration (the product form); fp64: plain")
@@ -593,7 +603,7 @@ def main():
     ap.add_argument("--maxit", type=int, default=None,
                     help="cap the GPLMR iterations (short runs for kernel profiling; not a bench value)")
     a = ap.parse_args()
-    if a.workload == "serve":
+    if a.workload in ("serve", "batch"):
         return serve_main(a)
     if a.workload in MATVEC:
         return matvec_main(a)
