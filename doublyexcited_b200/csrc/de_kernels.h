@@ -59,8 +59,8 @@ cudaError_t hammult_pass_launch(const HamDev &h, const float2 *x, float2 *y, int
                                 cudaStream_t st, double2 shift = double2{0.0, 0.0});
 
 // Even/odd-split form of one pass (hammult_ev.cu) for the grids
-// hammult_ev_supported accepts (complex128: NN = 9..15; complex64: NN =
-// 9..21); shs is the diagonal shift times SCALE^2.
+// hammult_ev_supported accepts (complex128: NN = 9, 11; complex64: NN =
+// 9..17); shs is the diagonal shift times SCALE^2.
 bool hammult_ev_supported(int nn, bool fp64);
 cudaError_t hammult_ev_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,
                                    int pass, cudaStream_t st, double2 shs);

@@ -115,9 +115,10 @@ struct EvArgs {
 // ring slots: the next stage's copies run under the current stage's work),
 // LCH chunks per line transform (2 halves the line accumulators), MINB
 // resident CTAs per SM asked of the compiler, LT line threads: 0 = every
-// thread owns a k-line and takes line tasks too; LT > 0 = LT extra threads
-// take all line tasks while the owners keep only their accumulators (fewer
-// registers per thread for the large complex128 grids).
+// thread owns a k-line or takes a line task (threads added until no thread
+// has two tasks in a stage); -1 = owners only, looping over the line tasks;
+// LT > 0 = LT extra threads take all line tasks while the owners keep only
+// their accumulators.
 template <class R, int NN, int MODE>
 struct EvShape;
 
@@ -133,25 +134,17 @@ EV_SHAPE(float, 9, 0, 4, 2, 1, 1, 0)
 EV_SHAPE(float, 9, 1, 1, 5, 1, 3, 0)
 EV_SHAPE(float, 11, 0, 4, 2, 1, 1, 0)
 EV_SHAPE(float, 11, 1, 1, 3, 1, 3, 0)
-EV_SHAPE(float, 13, 0, 2, 3, 1, 2, 0)
+EV_SHAPE(float, 13, 0, 4, 2, 1, 1, 0)
 EV_SHAPE(float, 13, 1, 1, 4, 1, 2, 0)
 EV_SHAPE(float, 15, 0, 2, 4, 1, 1, 0)
 EV_SHAPE(float, 15, 1, 1, 4, 1, 2, 0)
 EV_SHAPE(float, 17, 0, 2, 3, 1, 1, 0)
 EV_SHAPE(float, 17, 1, 1, 3, 1, 1, 0)
-EV_SHAPE(float, 19, 0, 1, 5, 1, 1, 0)
-EV_SHAPE(float, 19, 1, 1, 5, 1, 1, 0)
-EV_SHAPE(float, 21, 0, 1, 4, 1, 1, 0)
-EV_SHAPE(float, 21, 1, 1, 4, 1, 1, 0)
-// FP64 (complex128); NN >= 17 runs on the streaming kernels (hammult.cu)
+// FP64 (complex128); larger grids run on the streaming kernels (hammult.cu)
 EV_SHAPE(double, 9, 0, 2, 2, 1, 1, 0)
 EV_SHAPE(double, 9, 1, 1, 5, 1, 2, 0)
 EV_SHAPE(double, 11, 0, 2, 2, 1, 1, 0)
 EV_SHAPE(double, 11, 1, 1, 3, 1, 2, 0)
-EV_SHAPE(double, 13, 0, 2, 2, 1, 1, 0)
-EV_SHAPE(double, 13, 1, 1, 3, 1, 1, 0)
-EV_SHAPE(double, 15, 0, 1, 4, 1, 1, 0)
-EV_SHAPE(double, 15, 1, 1, 4, 1, 1, 0)
 #undef EV_SHAPE
 
 template <class R, int NN, int MODE>
@@ -168,13 +161,17 @@ struct EvCfg {
     // threads: LT > 0: owners + LT line threads; else enough that every
     // thread takes at most one line task per stage (the slowest thread of a
     // stage sets its time)
-    static constexpr int T = LT > 0 ? TO + LT : (TASKS > UNIT ? (TASKS + 31) / 32 * 32 : TO);
+    // (LT < 0: owners only, looping over the line tasks)
+    static constexpr int T = LT > 0 ? TO + LT : (LT == 0 && TASKS > UNIT ? (TASKS + 31) / 32 * 32 : TO);
     static constexpr int NST = (STEPS + GP - 1) / GP;  // stages per unit
-    static constexpr int XPL = MODE == 1 ? 4 : 2;      // planes per step: x+, x- (pass B: y+, y- too)
+    // planes per step: x+, x-, then pass A: V12(q+ - p), V12(q- - p) (in the
+    // real part) and pass B: pass A's partial y+, y-
+    static constexpr int XPL = 4;
     static constexpr int SLOT = GP * XPL;              // planes per ring slot
     static constexpr int DPL = GP * 4;                 // line-output planes [GP][u,w][i,j]
     static constexpr int T1A = MODE == 0 ? M : 0;      // A*TINV(r_q) copy (pass A)
     static constexpr size_t SMEM = (size_t)(2 * SLOT + DPL) * UNIT * sizeof(CX<R>) + (size_t)T1A * sizeof(R);
+    static_assert(SMEM <= 227 * 1024, "launch shape needs more shared memory than a CTA may have");
     static constexpr int LINES = PB * NN;              // lines per (step, dir, u/w, chunk)
     static constexpr int CHW = (N + 1 + LCH - 1) / LCH;  // outputs a per chunk
     // element offset of slab k from a thread's base (pass A: rows M apart)
@@ -202,6 +199,14 @@ __device__ __forceinline__ void cpa(CX<R> *s, const CX<R> *g)
 {
     if constexpr (sizeof(R) == 8) cpa16(s, g);
     else cpa8(s, g);
+}
+// one real (into the real part of a complex slot)
+template <class R>
+__device__ __forceinline__ void cpa_real(CX<R> *s, const R *g)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+    if constexpr (sizeof(R) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(g) : "memory");
 }
 
 // Owner index o -> (p_sub, ij).  Pass A keeps adjacent p in adjacent lanes
@@ -274,6 +279,7 @@ __device__ __forceinline__ void issue_stage(const UnitView<R> &v, CX<R> *slot)
             const int k = s == 0 ? C::N + b : C::N - b;
             cpa<R>(slot + (g * C::XPL + s) * C::UNIT + o, v.xb + k * C::KS);
             if constexpr (MODE == 1) cpa<R>(slot + (g * C::XPL + 2 + s) * C::UNIT + o, v.yb + k * C::KS);
+            else cpa_real<R>(slot + (g * C::XPL + 2 + s) * C::UNIT + o, v.v12b + (2 * NN - 1) * (2 * NN - 1) * k);
         }
     }
 }
@@ -365,6 +371,7 @@ __device__ __forceinline__ void line_tasks(const HamDev &h, const CX<R> *slot, C
     // task order (dir, chunk, step, u/w, line): the direction and chunk pick
     // different compiled code, so they change only between long runs of
     // tasks and few warps straddle two of them
+#pragma unroll 1
     for (int tau = threadIdx.x - T0; tau < NT; tau += TS) {
         const int la = tau % C::LINES;
         int r = tau / C::LINES;
@@ -420,8 +427,8 @@ __device__ __forceinline__ void acc_pair(Acc<R, NN> &A, R pr, R pi, R mr, R mi)
 // Owner phase 1 of step B: k-axis products, the potential term (pass A) and
 // the previous partial result brought to the accumulators' scale (pass B).
 template <class R, int NN, int MODE, int B>
-__device__ __forceinline__ void owner_k(const HamDev &h, Acc<R, NN> &A, const CX<R> *step, int o, R vp, R vm,
-                                        R shr, R shi, R sc2r, R sc2i)
+__device__ __forceinline__ void owner_k(const HamDev &h, Acc<R, NN> &A, const CX<R> *step, int o, const R *t1as,
+                                        int ij, R t1p, R shr, R shi, R sc2r, R sc2i)
 {
     using C = EvCfg<R, NN, MODE>;
     constexpr int N = NN / 2;
@@ -447,6 +454,8 @@ __device__ __forceinline__ void owner_k(const HamDev &h, Acc<R, NN> &A, const CX
     if constexpr (MODE == 0) {
         // V(p,q) (hammod.F90:576-578) times SCALE (the final 1/SCALE^2 leaves
         // V/SCALE, initmod.F90:224) plus the shift times SCALE^2
+        const R vp = (t1as[ij + C::P2 * (N + B)] + t1p) + step[2 * C::UNIT + o].x;
+        const R vm = B > 0 ? (t1as[ij + C::P2 * (N - B)] + t1p) + step[3 * C::UNIT + o].x : R(0);
         const R sre = (R)h.sre, sim = (R)h.sim;
         const R pr = fma(vp, sre, shr), pi = fma(vp, sim, shi);
         const R qr = fma(vm, sre, shr), qi = fma(vm, sim, shi);
@@ -479,14 +488,13 @@ __device__ __forceinline__ void owner_lines(Acc<R, NN> &A, const CX<R> *dstep, i
 }
 
 template <class R, int NN, int MODE, int B0, int G, int GN>
-__device__ __forceinline__ void owner_k_all(const HamDev &h, Acc<R, NN> &A, const CX<R> *slot, int o,
-                                            const R (&vpre)[GN][2], R shr, R shi, R sc2r, R sc2i)
+__device__ __forceinline__ void owner_k_all(const HamDev &h, Acc<R, NN> &A, const CX<R> *slot, int o, const R *t1as,
+                                            int ij, R t1p, R shr, R shi, R sc2r, R sc2i)
 {
     using C = EvCfg<R, NN, MODE>;
     if constexpr (G < GN) {
-        owner_k<R, NN, MODE, B0 + G>(h, A, slot + G * C::XPL * C::UNIT, o, vpre[G][0], vpre[G][1], shr, shi, sc2r,
-                                     sc2i);
-        owner_k_all<R, NN, MODE, B0, G + 1, GN>(h, A, slot, o, vpre, shr, shi, sc2r, sc2i);
+        owner_k<R, NN, MODE, B0 + G>(h, A, slot + G * C::XPL * C::UNIT, o, t1as, ij, t1p, shr, shi, sc2r, sc2i);
+        owner_k_all<R, NN, MODE, B0, G + 1, GN>(h, A, slot, o, t1as, ij, t1p, shr, shi, sc2r, sc2i);
     }
 }
 
@@ -521,28 +529,8 @@ __device__ __forceinline__ void stages(const HamDev &h, const EvArgs<R> &a, CX<R
             issue_stage<R, NN, MODE, 0>(unit_view<R, NN, MODE>(h, a, unext, psub, ij, o < C::UNIT), other);
         }
         cpa_commit();
-        // potential values of the stage's elements, loaded ahead of the line
-        // work so that their latency hides behind it
-        R vpre[GN][2];
-#pragma unroll
-        for (int g = 0; g < GN; ++g) vpre[g][0] = vpre[g][1] = R(0);
-        if constexpr (MODE == 0) {
-            if (cur.valid) {
-#pragma unroll
-                for (int g = 0; g < GN; ++g) {
-                    const int b = B0 + g;
-#pragma unroll
-                    for (int s = 0; s < 2; ++s) {
-                        const int k = s == 0 ? C::N + b : C::N - b;
-                        if (s == 0 || b > 0)
-                            vpre[g][s] = (t1as[ij + C::P2 * k] + cur.t1p) +
-                                         __ldg(cur.v12b + (2 * NN - 1) * (2 * NN - 1) * k);
-                    }
-                }
-            }
-        }
         line_tasks<R, NN, MODE, B0, GN>(h, slot, dpl);
-        if (o < C::UNIT) owner_k_all<R, NN, MODE, B0, 0, GN>(h, A, slot, o, vpre, shr, shi, sc2r, sc2i);
+        if (o < C::UNIT) owner_k_all<R, NN, MODE, B0, 0, GN>(h, A, slot, o, t1as, ij, cur.t1p, shr, shi, sc2r, sc2i);
         __syncthreads();
         if (o < C::UNIT) owner_lines_all<R, NN, MODE, B0, 0, GN>(A, dpl, o);
         stages<R, NN, MODE, ST + 1>(h, a, ring, dpl, t1as, A, cur, unext, sbase, o, psub, ij, shr, shi, sc2r, sc2i);
@@ -670,7 +658,7 @@ cudaError_t ev_dispatch(const HamDev &h, const CX<R> *x, CX<R> *y, int nvec, int
 {
 #define EV_CASE(NNV)                                                                       \
     case NNV:                                                                              \
-        if constexpr (sizeof(R) == 8 && NNV > 15) return cudaErrorInvalidValue;            \
+        if constexpr (NNV > (sizeof(R) == 8 ? 11 : 17)) return cudaErrorInvalidValue;      \
         else                                                                               \
             return pass == 0 ? ev_launch<R, NNV, 0>(h, x, y, nvec, vstride, shs, st)       \
                              : ev_launch<R, NNV, 1>(h, x, y, nvec, vstride, shs, st);
@@ -683,8 +671,6 @@ cudaError_t ev_dispatch(const HamDev &h, const CX<R> *x, CX<R> *y, int nvec, int
         EV_CASE(13)
         EV_CASE(15)
         EV_CASE(17)
-        EV_CASE(19)
-        EV_CASE(21)
 #endif
     default: return cudaErrorInvalidValue;
     }
@@ -693,7 +679,9 @@ cudaError_t ev_dispatch(const HamDev &h, const CX<R> *x, CX<R> *y, int nvec, int
 
 }  // namespace
 
-bool hammult_ev_supported(int nn, bool fp64) { return nn >= 9 && nn <= (fp64 ? 15 : 21); }
+// Grids where these kernels beat the streaming / cube kernels on B200 (block
+// matvec timings at N = 4..10): complex64 NN = 9..17, complex128 NN = 9, 11.
+bool hammult_ev_supported(int nn, bool fp64) { return nn >= 9 && nn <= (fp64 ? 11 : 17); }
 
 cudaError_t hammult_ev_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,
                                    int pass, cudaStream_t st, double2 shs)

@@ -146,11 +146,12 @@ DE_API int de_set_stream(de_problem *h, void *cuda_stream);
  * The reference times phases with MPI_WTIME (gplmr.F90:42-57). */
 DE_API int de_set_profiling(de_problem *h, int on);
 /* Which matvec kernels a handle uses: DE_MATVEC_FMA (the default) the
- * CUDA-core kernels on even/odd-split contractions for NN = 9..21,
- * DE_MATVEC_TENSOR the axis contractions on the FP64 tensor cores (DMMA)
- * for NN = 9..19, DE_MATVEC_STREAM the earlier CUDA-core streaming kernels
- * for NN = 13..19 (kept for comparison).  Other grids use the shared-memory
- * cube kernels whatever the choice.  All give the reference's H x to
+ * fastest CUDA-core kernels per grid: even/odd-split contractions for the
+ * mixed form's complex64 matvec at NN = 9..17 and the plain form's at NN =
+ * 9, 11, streaming kernels at NN = 13..19 otherwise, shared-memory cube
+ * kernels elsewhere; DE_MATVEC_TENSOR the axis contractions on the FP64
+ * tensor cores (DMMA) for NN = 9..19; DE_MATVEC_STREAM the streaming / cube
+ * kernels everywhere (for comparison).  All give the reference's H x to
  * rounding. */
 enum { DE_MATVEC_FMA = 0, DE_MATVEC_TENSOR = 1, DE_MATVEC_STREAM = 2 };
 DE_API int de_set_matvec_kernel(de_problem *h, int kind);

@@ -239,11 +239,11 @@ def test_block_matvec_config_matches_oracle(de, oracle, n):
 
 @pytest.mark.parametrize("n", [4, 5, 6, 7, 8, 9, 10])
 def test_even_odd_kernels_match_streaming_kernels(de, n):
-    """The even/odd-split kernels (the default) against the earlier
-    streaming / cube kernels on a block of two vectors with a fused shift,
-    FP64 within 1e-13 and FP32 within 1e-6 relative; N=4..10 covers every
-    grid the even/odd kernels serve (NN = 9..21) and both passes' partial
-    last units."""
+    """The default kernels (even/odd-split where they are faster) against
+    the streaming / cube kernels on a block of two vectors with a fused
+    shift, FP64 within 1e-13 and FP32 within 1e-6 relative; N=4..10 covers
+    every grid the even/odd kernels serve and both passes' partial last
+    units."""
     import torch
 
     with de.Problem(n=n, delta=2.0, theta=0.3) as g64, \
