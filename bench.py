@@ -138,7 +138,9 @@ def run_served(de, seeded_start, cfg, precision, workers=None):
     return {"solves_per_s": len(reqs) / t_end, "wall_s": t_end, "p50_s": float(np.percentile(lat, 50)),
             "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "ok": int(sum(ok)),
             "converged": int(sum(conv)), "e": {i: done[i].e.copy() for i in range(len(reqs))},
-            "conv": {i: bool(done[i].converged and done[i].status == 0) for i in range(len(reqs))}}
+            "conv": {i: bool(done[i].converged and done[i].status == 0) for i in range(len(reqs))},
+            "not_converged": [dict(reqs[i], status=int(done[i].status)) for i in range(len(reqs))
+                              if not (done[i].converged and done[i].status == 0)]}
 
 
 def hammults_per_solve(w, iters):

@@ -1221,6 +1221,133 @@ cudaError_t gram_launch(const ColListF &L, const ColListF &R, int64_t len, int h
     return gram_any(L, R, len, herm, out, ldo, work, st);
 }
 
+namespace {
+// Hermitian Gram Z^H Z of n <= 7 vectors (28 packed upper-triangle sums).
+// Each row is read once per thread pair: the two threads of a pair take
+// the first and the second 14 sums of the same rows, so a thread keeps 14
+// FP64 complex accumulators; every thread has two rows in flight.  Warp
+// shuffles reduce the even and odd lanes separately, then the block, then
+// the last block sums the per-block partials in a fixed order.
+constexpr int kHermNZ = 7, kHermNP = kHermNZ * (kHermNZ + 1) / 2, kHermHalf = kHermNP / 2;
+
+__host__ __device__ constexpr int herm_i(int k)
+{
+    int i = 0;
+    while (k >= kHermNZ - i) {
+        k -= kHermNZ - i;
+        ++i;
+    }
+    return i;
+}
+__host__ __device__ constexpr int herm_j(int k)
+{
+    int i = 0;
+    while (k >= kHermNZ - i) {
+        k -= kHermNZ - i;
+        ++i;
+    }
+    return i + k;
+}
+
+// the 14 sums of one half (PART) over two rows
+// the 14 sums of one half (PART) over two rows; K walks them at compile time
+template <int PART, int K>
+__device__ __forceinline__ void herm_acc(double (&ar)[kHermHalf], double (&ai)[kHermHalf], const float2 (&z0)[kHermNZ],
+                                         const float2 (&z1)[kHermNZ])
+{
+    if constexpr (K < kHermHalf) {
+        constexpr int i = herm_i(PART * kHermHalf + K), j = herm_j(PART * kHermHalf + K);
+        // conj(z_i) z_j; products of two floats are exact in double
+        ar[K] = fma((double)z0[i].x, (double)z0[j].x, ar[K]);
+        ar[K] = fma((double)z0[i].y, (double)z0[j].y, ar[K]);
+        ai[K] = fma((double)z0[i].x, (double)z0[j].y, ai[K]);
+        ai[K] = fma(-(double)z0[i].y, (double)z0[j].x, ai[K]);
+        ar[K] = fma((double)z1[i].x, (double)z1[j].x, ar[K]);
+        ar[K] = fma((double)z1[i].y, (double)z1[j].y, ar[K]);
+        ai[K] = fma((double)z1[i].x, (double)z1[j].y, ai[K]);
+        ai[K] = fma(-(double)z1[i].y, (double)z1[j].x, ai[K]);
+        herm_acc<PART, K + 1>(ar, ai, z0, z1);
+    }
+}
+
+__global__ void __launch_bounds__(256, 2)
+    gram_herm_kernel(const __grid_constant__ ColListT<float2> Z, int64_t len, double2 *__restrict__ work,
+                     double2 *__restrict__ out, int ldo)
+{
+    const int n = Z.n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int part = warp & 1;  // the two warps of a pair read the same rows
+    double ar[kHermHalf], ai[kHermHalf];
+#pragma unroll
+    for (int k = 0; k < kHermHalf; ++k) ar[k] = ai[k] = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * (blockDim.x >> 1);
+    const int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 6) + (warp >> 1)) * 32 + lane;
+    for (int64_t r0 = base; r0 < len; r0 += 2 * stride) {
+        const int64_t r1 = r0 + stride;
+        float2 z0[kHermNZ], z1[kHermNZ];
+#pragma unroll
+        for (int j = 0; j < kHermNZ; ++j) {
+            z0[j] = (j < n) ? __ldg(Z.a[j] + r0) : make_float2(0.f, 0.f);
+            z1[j] = (j < n && r1 < len) ? __ldg(Z.a[j] + r1) : make_float2(0.f, 0.f);
+        }
+        if (part == 0) herm_acc<0, 0>(ar, ai, z0, z1);
+        else herm_acc<1, 0>(ar, ai, z0, z1);
+    }
+    // reduce each warp, then the warps of each parity
+    __shared__ double2 wsum[8][kHermHalf];
+#pragma unroll
+    for (int k = 0; k < kHermHalf; ++k) {
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            ar[k] += __shfl_xor_sync(0xffffffffu, ar[k], off);
+            ai[k] += __shfl_xor_sync(0xffffffffu, ai[k], off);
+        }
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < kHermHalf; ++k) wsum[warp][k] = make_double2(ar[k], ai[k]);
+    }
+    __syncthreads();
+    unsigned *ticket = reinterpret_cast<unsigned *>(work);
+    double2 *part_out = work + 1;
+    const int nw = blockDim.x >> 5;
+    if (threadIdx.x < kHermNP) {
+        const int pp = threadIdx.x / kHermHalf, k = threadIdx.x % kHermHalf;
+        double2 t = make_double2(0.0, 0.0);
+        for (int w = pp; w < nw; w += 2) {
+            t.x += wsum[w][k].x;
+            t.y += wsum[w][k].y;
+        }
+        part_out[(int64_t)blockIdx.x * kHermNP + threadIdx.x] = t;
+    }
+    if (last_block(ticket, gridDim.x)) {
+        __shared__ double2 res[32];
+        reduce_partials(part_out, gridDim.x, kHermNP, kHermNP, res);
+        for (int o = threadIdx.x; o < n * n; o += blockDim.x) {
+            const int i = o % n, j = o / n;
+            const int a = i < j ? i : j, b = i < j ? j : i;
+            const int kk = a * kHermNZ - a * (a - 1) / 2 + (b - a);  // packed index of (a, b)
+            double2 v = res[kk];
+            if (i > j) v.y = -v.y;
+            out[i + (int64_t)ldo * j] = v;
+        }
+        if (threadIdx.x == 0) *ticket = 0u;
+    }
+}
+}  // namespace
+
+cudaError_t gram_herm_launch(const ColListF &Z, int64_t len, double2 *out, int ldo, double2 *work, cudaStream_t st)
+{
+    if (Z.n < 1 || Z.n > kHermNZ || len < 1) return cudaErrorInvalidValue;
+    // partials: 28 per block must fit the reduction scratch (kSmallBlocks * 32)
+    const int64_t want = (len + 511) / 512;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min(wave_blocks<gram_herm_kernel>(),
+                                                                                  kSmallBlocks)));
+    gram_herm_kernel<<<blocks, 256, 0, st>>>(Z, len, work, out, ldo);
+    count_launch();
+    return cudaGetLastError();
+}
+
 template <class SI, class SO>
 static cudaError_t update_any(const UpdListT<SI, SO> &U, const double2 *c_dev, int ldc, int64_t len, cudaStream_t st)
 {

@@ -101,6 +101,10 @@ cudaError_t gram_launch(const ColList &L, const ColList &R, int64_t len, int her
 cudaError_t gram_launch(const ColListF &L, const ColListF &R, int64_t len, int herm, double2 *out, int ldo,
                         double2 *work, cudaStream_t st);
 
+// Hermitian Gram G = Z^H Z of n <= 7 complex64 vectors (FP64 sums), all n x n
+// entries written to DEVICE out (column-major, ldo); work as for gram.
+cudaError_t gram_herm_launch(const ColListF &Z, int64_t len, double2 *out, int ldo, double2 *work, cudaStream_t st);
+
 // Y_j = beta_j * Y_j + alpha * sum_i X_i C(i,j) for j < nout (nout <= 16,
 // nin <= kMaxCols); C is DEVICE memory (complex, column-major, ldc).  Each
 // row is read before it is written, so Y may alias X columns.

@@ -814,7 +814,24 @@ struct Solver {
             DE_TRY(mult_shifted<float2>(Z32 + (int64_t)(i - 1) * k * D, Z32 + (int64_t)i * k * D, k));
         mv_ref += (order + 1) * k;  // the reference forms (2 order + 1) k products
         std::vector<cplx> g;  // [Z_1..Z_order]^H [Z_0..Z_order], nq x nz
-        DE_TRY(gram_hostT(colsT(Z32 + (int64_t)k * D, nq, D), colsT(Z32, nz, D), g));
+        if (k == 1 && nz <= 7) {
+            // one column: the Hermitian Gram of the nz basis vectors, read once
+            cudaError_t e = gram_herm_launch(colsT(Z32, nz, D), D, dG, nz, h->d_work, st);
+            if (e != cudaSuccess) return cuda_error(e, "gram_herm");
+            DE_CUDA(cudaMemcpyAsync(hbuf, dG, (size_t)nz * nz * sizeof(double2), cudaMemcpyDeviceToHost, st));
+            int *hf = reinterpret_cast<int *>(hbuf + (size_t)nz * nz);
+            DE_CUDA(cudaMemcpyAsync(hf, dFlags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            DE_CUDA(cudaStreamSynchronize(st));
+            DE_TRY(check_flags(hf[1]));
+            g.resize((size_t)nq * nz);
+            for (int j = 0; j < nz; ++j)
+                for (int i = 0; i < nq; ++i) {
+                    const double2 v = hbuf[(i + 1) + (size_t)nz * j];
+                    g[i + (size_t)nq * j] = cplx(v.x, v.y);
+                }
+        } else {
+            DE_TRY(gram_hostT(colsT(Z32 + (int64_t)k * D, nq, D), colsT(Z32, nz, D), g));
+        }
         auto t0 = clk::now();
         std::vector<cplx> a;
         DE_TRY(minres_normal(nq, k, g, a));
