@@ -1512,6 +1512,79 @@ cudaError_t gs_pass2_launch(const float2 *const *qp, const float2 *const *vp, in
     return gs_pass2_go(qp, vp, m, q, v, d2, len, cout, st);
 }
 
+// The mixed inner solve's normal equations for one column: from the
+// Hermitian Gram G of the power basis z_0..z_nq (nz = nq + 1 <= 8,
+// column-major, ld nz), with D = sqrt(diag(G[1:,1:])), solves
+// (D^-1 G[1:,1:] D^-1 + 1e-13 I) y = D^-1 G[1:,0] by Cholesky and returns
+// a = D^-1 y (nq values).  Flag 8 if the system is not positive definite.
+__global__ void small_sstep_solve(const double2 *__restrict__ G, int nz, double2 *__restrict__ a, int *flag)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int n = nz - 1;
+    double d[8];
+    double2 R[8 * 8], y[8];
+    for (int i = 0; i < n; ++i) {
+        const double v = G[(i + 1) + nz * (i + 1)].x;
+        if (!(v > 0.0) || !isfinite(v)) {
+            raise_flag(flag, 8);
+            return;
+        }
+        d[i] = sqrt(v);
+    }
+    // Cholesky of the scaled, regularised Gram: Gs = R^H R (R upper)
+    for (int j = 0; j < n; ++j) {
+        double dj = G[(j + 1) + nz * (j + 1)].x / (d[j] * d[j]) + 1e-13;
+        for (int i = 0; i < j; ++i) dj -= R[i + 8 * j].x * R[i + 8 * j].x + R[i + 8 * j].y * R[i + 8 * j].y;
+        if (!(dj > 0.0) || !isfinite(dj)) {
+            raise_flag(flag, 8);
+            return;
+        }
+        const double rjj = sqrt(dj);
+        R[j + 8 * j] = make_double2(rjj, 0.0);
+        for (int l = j + 1; l < n; ++l) {
+            const double2 g = G[(j + 1) + nz * (l + 1)];
+            double2 t = make_double2(g.x / (d[j] * d[l]), g.y / (d[j] * d[l]));
+            for (int i = 0; i < j; ++i) {  // t -= conj(R(i,j)) R(i,l)
+                const double2 p = R[i + 8 * j], q = R[i + 8 * l];
+                t.x -= p.x * q.x + p.y * q.y;
+                t.y -= p.x * q.y - p.y * q.x;
+            }
+            R[j + 8 * l] = make_double2(t.x / rjj, t.y / rjj);
+        }
+    }
+    // R^H y = D^-1 G[1:, 0] (forward), then R x = y (back)
+    for (int i = 0; i < n; ++i) {
+        const double2 g = G[(i + 1) + nz * 0];
+        double2 t = make_double2(g.x / d[i], g.y / d[i]);
+        for (int l = 0; l < i; ++l) {  // t -= conj(R(l,i)) y(l)
+            const double2 p = R[l + 8 * i], q = y[l];
+            t.x -= p.x * q.x + p.y * q.y;
+            t.y -= p.x * q.y - p.y * q.x;
+        }
+        const double rii = R[i + 8 * i].x;
+        y[i] = make_double2(t.x / rii, t.y / rii);
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double2 t = y[i];
+        for (int l = i + 1; l < n; ++l) {  // t -= R(i,l) x(l)
+            const double2 p = R[i + 8 * l], q = y[l];
+            t.x -= p.x * q.x - p.y * q.y;
+            t.y -= p.x * q.y + p.y * q.x;
+        }
+        const double rii = R[i + 8 * i].x;
+        y[i] = make_double2(t.x / rii, t.y / rii);
+    }
+    for (int i = 0; i < n; ++i) a[i] = make_double2(y[i].x / d[i], y[i].y / d[i]);
+}
+
+cudaError_t small_sstep_solve_launch(const double2 *g, int nz, double2 *a, int *flag, cudaStream_t st)
+{
+    if (nz < 2 || nz > 9) return cudaErrorInvalidValue;
+    small_sstep_solve<<<1, 32, 0, st>>>(g, nz, a, flag);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t small_cholinv_launch(const double2 *g, int k, double2 *rinv, int *flag, cudaStream_t st)
 {
     if (k < 1 || k > 16) return cudaErrorInvalidValue;

@@ -172,6 +172,9 @@ cudaError_t to_f32_launch(const double *x, float *y, int64_t n, cudaStream_t st)
 // flag bits: 1 Cholesky breakdown, 2 all-zero block, 4 orthonormality
 // self-check failed, 8 singular 1 x 1 Gram.
 cudaError_t small_cholinv_launch(const double2 *g, int k, double2 *rinv, int *flag, cudaStream_t st);
+// The mixed inner solve's normal equations for one column (Gram g of the
+// nz <= 9 power-basis vectors): the nz - 1 coefficients into DEVICE a.
+cudaError_t small_sstep_solve_launch(const double2 *g, int nz, double2 *a, int *flag, cudaStream_t st);
 cudaError_t small_hsqrt1_launch(const double2 *g, double2 *ginvh, double2 *gsq, int *flag, cudaStream_t st);
 // |T - I| <= tol elementwise (the reference's self-check uses 1e-10).
 cudaError_t small_ortho_check_launch(const double2 *t, int k, int *flag, cudaStream_t st, double tol = 1e-10);

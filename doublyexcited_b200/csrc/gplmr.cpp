@@ -798,11 +798,11 @@ struct Solver {
     // solution is Y = [Z_0 .. Z_order-1] a with (Q^H Q) a = Q^H B, so one Gram
     // of the Z blocks (FP64 sums over complex64 vectors) and one update
     // replace the Gram-Schmidt passes: about 20 vector passes per call
-    // instead of about 120 at NEV = 1.  The normal equations are solved on
-    // the host after diagonal scaling through an SVD that drops singular
-    // values below 1e-13 of the largest (the basis is far from orthogonal;
-    // this is a preconditioner, and the FP64 outer iteration refines every
-    // Ritz pair).
+    // instead of about 120 at NEV = 1.  The normal equations are solved
+    // after diagonal scaling with a 1e-13 ridge by Cholesky -- on the device
+    // for one column, on the host for a block (the basis is far from
+    // orthogonal; this is a preconditioner, and the FP64 outer iteration
+    // refines every Ritz pair).
     int basic_sstep(double2 *b, int k)
     {
         const int nq = order * k, nz = (order + 1) * k;
@@ -813,25 +813,17 @@ struct Solver {
         for (int i = 1; i <= order; ++i)
             DE_TRY(mult_shifted<float2>(Z32 + (int64_t)(i - 1) * k * D, Z32 + (int64_t)i * k * D, k));
         mv_ref += (order + 1) * k;  // the reference forms (2 order + 1) k products
-        std::vector<cplx> g;  // [Z_1..Z_order]^H [Z_0..Z_order], nq x nz
         if (k == 1 && nz <= 7) {
-            // one column: the Hermitian Gram of the nz basis vectors, read once
+            // one column: the Hermitian Gram of the nz basis vectors (read
+            // once) and the normal equations on the device -- no host trip
             cudaError_t e = gram_herm_launch(colsT(Z32, nz, D), D, dG, nz, h->d_work, st);
             if (e != cudaSuccess) return cuda_error(e, "gram_herm");
-            DE_CUDA(cudaMemcpyAsync(hbuf, dG, (size_t)nz * nz * sizeof(double2), cudaMemcpyDeviceToHost, st));
-            int *hf = reinterpret_cast<int *>(hbuf + (size_t)nz * nz);
-            DE_CUDA(cudaMemcpyAsync(hf, dFlags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
-            DE_CUDA(cudaStreamSynchronize(st));
-            DE_TRY(check_flags(hf[1]));
-            g.resize((size_t)nq * nz);
-            for (int j = 0; j < nz; ++j)
-                for (int i = 0; i < nq; ++i) {
-                    const double2 v = hbuf[(i + 1) + (size_t)nz * j];
-                    g[i + (size_t)nq * j] = cplx(v.x, v.y);
-                }
-        } else {
-            DE_TRY(gram_hostT(colsT(Z32 + (int64_t)k * D, nq, D), colsT(Z32, nz, D), g));
+            if ((e = small_sstep_solve_launch(dG, nz, dSV, dFlags, st)) != cudaSuccess)
+                return cuda_error(e, "small_sstep_solve");
+            return updateT(Z32, nq, b, 1, dSV, nq);
         }
+        std::vector<cplx> g;  // [Z_1..Z_order]^H [Z_0..Z_order], nq x nz
+        DE_TRY(gram_hostT(colsT(Z32 + (int64_t)k * D, nq, D), colsT(Z32, nz, D), g));
         auto t0 = clk::now();
         std::vector<cplx> a;
         DE_TRY(minres_normal(nq, k, g, a));
@@ -840,8 +832,10 @@ struct Solver {
         return updateT(Z32, nq, b, k, dC, nq);
     }
 
-    // Solves (Q^H Q) a = Q^H B from g = Q^H [B Q] (nq x (k + nq)): diagonal
-    // scaling, then the pseudo-inverse of the scaled Gram from zgesdd.
+    // Solves (Q^H Q) a = Q^H B from g = Q^H [B Q] (nq x (k + nq)): with
+    // D = sqrt(diag(Q^H Q)), (D^-1 Q^H Q D^-1 + 1e-13 I) y = D^-1 Q^H B by
+    // Cholesky (zpotrf), a = D^-1 y -- the same regularised system as the
+    // device solve of one column.
     int minres_normal(int nq, int k, const std::vector<cplx> &g, std::vector<cplx> &a)
     {
         const Lapack &L = lapack();
@@ -851,26 +845,27 @@ struct Solver {
             if (!(v > 0.0) || !std::isfinite(v)) return set_error(DE_E_NAN, "inner-solve basis vector %d is zero", i);
             d[i] = std::sqrt(v);
         }
-        std::vector<cplx> gs((size_t)nq * nq), u((size_t)nq * nq), vt((size_t)nq * nq);
+        std::vector<cplx> r((size_t)nq * nq);
         for (int j = 0; j < nq; ++j)
-            for (int i = 0; i < nq; ++i) gs[i + (size_t)nq * j] = g[i + (size_t)nq * (k + j)] / (d[i] * d[j]);
-        std::vector<double> sv(nq), rwork(20 * nq * nq + 100);
-        std::vector<cplx> zwork(20 * nq * nq + 100);
-        std::vector<int> iwork(100 * nq);
-        const int lwork = (int)zwork.size();
+            for (int i = 0; i < nq; ++i)
+                r[i + (size_t)nq * j] = g[i + (size_t)nq * (k + j)] / (d[i] * d[j]) + (i == j ? 1e-13 : 0.0);
         int info = 0;
-        L.zgesdd("A", &nq, &nq, gs.data(), &nq, sv.data(), u.data(), &nq, vt.data(), &nq, zwork.data(), &lwork,
-                 rwork.data(), iwork.data(), &info, 1);
-        if (info != 0) return set_error(DE_E_SVD, "zgesdd info=%d", info);
+        L.zpotrf("U", &nq, r.data(), &nq, &info, 1);
+        if (info != 0) return set_error(DE_E_SVD, "inner-solve Gram matrix is not positive definite (zpotrf %d)", info);
         a.assign((size_t)nq * k, 0.0);
-        for (int l = 0; l < nq; ++l) {
-            if (!(sv[l] > 1e-13 * sv[0])) continue;
-            for (int j = 0; j < k; ++j) {
-                cplx t = 0.0;  // (u_l^H rhs_j) / s_l, rhs scaled by 1/d
-                for (int i = 0; i < nq; ++i) t += std::conj(u[i + (size_t)nq * l]) * g[i + (size_t)nq * j] / d[i];
-                t /= sv[l];
-                for (int i = 0; i < nq; ++i) a[i + (size_t)nq * j] += std::conj(vt[l + (size_t)nq * i]) * t / d[i];
+        for (int j = 0; j < k; ++j) {
+            std::vector<cplx> y(nq);
+            for (int i = 0; i < nq; ++i) {  // R^H y = D^-1 rhs
+                cplx t = g[i + (size_t)nq * j] / d[i];
+                for (int l = 0; l < i; ++l) t -= std::conj(r[l + (size_t)nq * i]) * y[l];
+                y[i] = t / r[i + (size_t)nq * i].real();
             }
+            for (int i = nq - 1; i >= 0; --i) {  // R x = y
+                cplx t = y[i];
+                for (int l = i + 1; l < nq; ++l) t -= r[i + (size_t)nq * l] * y[l];
+                y[i] = t / r[i + (size_t)nq * i].real();
+            }
+            for (int i = 0; i < nq; ++i) a[i + (size_t)nq * j] = y[i] / d[i];
         }
         return DE_OK;
     }

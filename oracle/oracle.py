@@ -375,9 +375,10 @@ def sstep_minres(x: np.ndarray, order: int, sigma: complex, mult, store=None) ->
     K_order(H, X) as basicblocklansolve, from the power basis Z_0 = X,
     Z_i = (H - sigma) Z_{i-1} and one Gram: with Q = [Z_1..Z_order] the
     solution is [Z_0..Z_order-1] a, (Q^H Q) a = Q^H X, solved after diagonal
-    scaling through an SVD that drops singular values below 1e-13 of the
-    largest.  `store` rounds every basis block as the library stores it
-    (complex64 in the mixed form)."""
+    scaling D with a 1e-13 ridge by Cholesky:
+    (D^-1 Q^H Q D^-1 + 1e-13 I) y = D^-1 Q^H X, a = D^-1 y.  `store` rounds
+    every basis block as the library stores it (complex64 in the mixed
+    form)."""
     k = x.shape[1]
     rnd = store if store is not None else (lambda v: v)
     z = [rnd(x)]
@@ -388,10 +389,10 @@ def sstep_minres(x: np.ndarray, order: int, sigma: complex, mult, store=None) ->
     g = q.conj().T @ zf
     gq, rhs = g[:, k:], g[:, :k]
     d = np.sqrt(np.real(np.diag(gq)))
-    u, sv, vh = np.linalg.svd(gq / d[:, None] / d[None, :])
-    keep = sv > 1e-13 * sv[0]
-    a = (vh[keep].conj().T / sv[keep]) @ (u[:, keep].conj().T @ (rhs / d[:, None]))
-    return zf[:, :order * k] @ (a / d[:, None])
+    gs = gq / d[:, None] / d[None, :] + 1e-13 * np.eye(gq.shape[0])
+    lo = np.linalg.cholesky(gs)
+    y = np.linalg.solve(lo.conj().T, np.linalg.solve(lo, rhs / d[:, None]))
+    return zf[:, :order * k] @ (y / d[:, None])
 
 
 # --------------------------------------------------------------------------
