@@ -165,9 +165,9 @@ def alg_bytes(nn):
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, pass A + pass B)
 # per vector-matvec of the kernels the library picks, keyed by (NN,
 # storage): one ncu capture of the block-of-2 matvec at N=6 (`--workload
-# matvec-n6`), both passes' bytes over 2 vectors: ev_kernel<float, 13> and
-# stream_kernel<double, 13>.  Grids without a capture report null.
-NCU_TRAFFIC_PER_VECTOR = {(13, "f32"): 149.4e6, (13, "f64"): 342.25e6}
+# matvec-n6`), both passes' bytes over 2 vectors: ev_kernel<float, 13>.
+# Kernels without a capture report null.
+NCU_TRAFFIC_PER_VECTOR = {(13, "f32"): 149.4e6}
 
 
 def solve_config(a, w):
@@ -312,10 +312,10 @@ def dist_setup():
 def matvec_kernel_name(nn, fp32):
     """The kernels the library picks for a grid (de_set_matvec_kernel's
     default): even/odd-split kernels for complex64 at NN 9..17 and
-    complex128 at NN 9, 11, streaming kernels at NN 13..19, cube kernels
+    complex128 at NN 9..13, streaming kernels at NN 15..19, cube kernels
     elsewhere."""
     r = "float" if fp32 else "double"
-    if 9 <= nn <= (17 if fp32 else 11):
+    if 9 <= nn <= (17 if fp32 else 13):
         return f"hammult ev_kernel<{r}, {nn}> pass A + pass B"
     if 13 <= nn <= 19:
         return f"hammult stream_kernel<{r}, {nn}> pass A + pass B"

@@ -944,6 +944,132 @@ int stream_blocks(int64_t len)
     return (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, 148 * 4));
 }
 
+// Reflection sectors.  The grid is symmetric under c -> nn-1-c of each
+// Cartesian axis (applied to both electrons at once), and H commutes with
+// the three reflections; they generate a group of 8 elements, indexed by a
+// 3-bit mask r (bit a: axis a reflected).  Its characters chi_c(r) =
+// (-1)^popcount(c & r) label 8 sectors.  Element index of a vector:
+// x1 + nn y1 + nn^2 z1 + nn^3 (x2 + nn y2 + nn^2 z2).
+__device__ __forceinline__ int64_t refl_image(const int c[6], int r, int nn)
+{
+    const int m = nn - 1;
+    int d[6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const bool f = (r >> a) & 1;
+        d[a] = f ? m - c[a] : c[a];
+        d[a + 3] = f ? m - c[a + 3] : c[a + 3];
+    }
+    const int64_t n1 = nn, n2 = n1 * nn, n3 = n2 * nn;
+    return d[0] + n1 * d[1] + n2 * d[2] + n3 * (d[3] + n1 * d[4] + n2 * d[5]);
+}
+
+// work[r * gridDim.x + block] = the block's share of <x, R_r x> =
+// sum_i conj(x_i) x_{R_r(i)}
+__global__ void __launch_bounds__(256) refl_corr_kernel(const double2 *__restrict__ x, int nn, int64_t d,
+                                                        double2 *__restrict__ work)
+{
+    double sr[8], si[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) sr[r] = si[r] = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d; i += stride) {
+        int c[6];
+        int64_t t = i;
+#pragma unroll
+        for (int a = 0; a < 5; ++a) {
+            c[a] = (int)(t % nn);
+            t /= nn;
+        }
+        c[5] = (int)t;
+        const double2 a = x[i];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const double2 b = x[refl_image(c, r, nn)];
+            sr[r] += a.x * b.x + a.y * b.y;
+            si[r] += a.x * b.y - a.y * b.x;
+        }
+    }
+    __shared__ double2 red[8][8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            sr[r] += __shfl_down_sync(0xffffffffu, sr[r], off);
+            si[r] += __shfl_down_sync(0xffffffffu, si[r], off);
+        }
+        if ((threadIdx.x & 31) == 0) red[r][threadIdx.x >> 5] = make_double2(sr[r], si[r]);
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            a += red[threadIdx.x][w].x;
+            b += red[threadIdx.x][w].y;
+        }
+        work[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = make_double2(a, b);
+    }
+}
+
+// 8-point Walsh-Hadamard transform in place: v[c] <- sum_r (-1)^popcount(c & r) v[r]
+__device__ __forceinline__ void wht8(double2 v[8])
+{
+#pragma unroll
+    for (int h = 1; h < 8; h <<= 1)
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+            if (!(r & h)) {
+                const double2 a = v[r], b = v[r | h];
+                v[r] = make_double2(a.x + b.x, a.y + b.y);
+                v[r | h] = make_double2(a.x - b.x, a.y - b.y);
+            }
+}
+
+// In-place projection onto the sectors whose bit is set in keep: one thread
+// per orbit of the group.  The orbit's canonical element has, on every axis,
+// its electron pair (c1, c2) with c1 < N, or c1 = N and c2 <= N (N = nn/2),
+// so there are K = N nn + N + 1 canonical pairs per axis and K^3 orbits.
+// The thread reads the orbit's 8 values, transforms them to the sector
+// components (wht8), zeroes the sectors not kept, transforms back (/8) and
+// writes the 8 values.  A pair (N, N) is its own reflection; the orbit then
+// repeats elements, and every copy of an element receives the same value.
+__global__ void __launch_bounds__(256) refl_project_kernel(double2 *__restrict__ x, int nn, unsigned keep)
+{
+    const int n = nn / 2, k = n * nn + n + 1;
+    const int64_t orbits = (int64_t)k * k * k;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < orbits; t += stride) {
+        int c[6];
+        int64_t u = t;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int q = (int)(u % k);
+            u /= k;
+            if (q < n * nn) {
+                c[a] = q % n;
+                c[a + 3] = q / n;
+            } else {
+                c[a] = n;
+                c[a + 3] = q - n * nn;
+            }
+        }
+        double2 v[8];
+        int64_t idx[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            idx[r] = refl_image(c, r, nn);
+            v[r] = x[idx[r]];
+        }
+        wht8(v);
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+            if (!((keep >> r) & 1)) v[r] = make_double2(0.0, 0.0);
+        wht8(v);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) x[idx[r]] = make_double2(0.125 * v[r].x, 0.125 * v[r].y);
+    }
+}
+
 }  // namespace
 
 int64_t gram_work_elems(int nl, int nr, int64_t len)
@@ -1642,6 +1768,30 @@ cudaError_t exch_project_launch(double2 *x, int64_t m, double s, cudaStream_t st
     const int64_t t = (m + 31) / 32;
     if (m < 1 || t > 65535) return cudaErrorInvalidValue;
     exch_kernel<true><<<dim3((unsigned)t, (unsigned)t), 256, 0, st>>>(x, m, s, nullptr);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t refl_corr_launch(const double2 *x, int nn, double2 *out, double2 *work, cudaStream_t st)
+{
+    if (nn < 3 || !(nn & 1)) return cudaErrorInvalidValue;
+    const int64_t d = (int64_t)nn * nn * nn * nn * nn * nn;
+    const int blocks = stream_blocks(d);
+    // work[0] is the fused reductions' ticket: the partials start at work + 1
+    refl_corr_kernel<<<blocks, 256, 0, st>>>(x, nn, d, work + 1);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    dotdiag_reduce<<<8, 256, 0, st>>>(work + 1, blocks, 8, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t refl_project_launch(double2 *x, int nn, unsigned keep, cudaStream_t st)
+{
+    if (nn < 3 || !(nn & 1) || keep > 255u) return cudaErrorInvalidValue;
+    const int64_t k = (int64_t)(nn / 2) * nn + nn / 2 + 1;
+    refl_project_kernel<<<stream_blocks(k * k * k), 256, 0, st>>>(x, nn, keep);
     count_launch();
     return cudaGetLastError();
 }

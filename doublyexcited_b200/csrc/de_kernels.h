@@ -59,7 +59,7 @@ cudaError_t hammult_pass_launch(const HamDev &h, const float2 *x, float2 *y, int
                                 cudaStream_t st, double2 shift = double2{0.0, 0.0});
 
 // Even/odd-split form of one pass (hammult_ev.cu) for the grids
-// hammult_ev_supported accepts (complex128: NN = 9, 11; complex64: NN =
+// hammult_ev_supported accepts (complex128: NN = 9..13; complex64: NN =
 // 9..17); shs is the diagonal shift times SCALE^2.
 bool hammult_ev_supported(int nn, bool fp64);
 cudaError_t hammult_ev_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,
@@ -163,6 +163,15 @@ cudaError_t gs_pass2_launch(const float2 *const *qp, const float2 *const *vp, in
 // projection X <- (X + s X^T)/2.
 cudaError_t exch_dot_launch(const double2 *x, int64_t m, double2 *out, double2 *work, cudaStream_t st);
 cudaError_t exch_project_launch(double2 *x, int64_t m, double s, cudaStream_t st);
+
+// Reflection sectors of one nn^6 vector (nn odd): out[r] = <x, R_r x> for
+// the 8 products R_r of the axis reflections c -> nn-1-c (bit a of r:
+// axis a, both electrons; work as for gram, >= 8 * 592 + 1 elements, work[0]
+// untouched), and the in-place
+// projection onto the sectors c with bit c of keep set, sector c being
+// the eigenspace where R_r has eigenvalue (-1)^popcount(c & r).
+cudaError_t refl_corr_launch(const double2 *x, int nn, double2 *out, double2 *work, cudaStream_t st);
+cudaError_t refl_project_launch(double2 *x, int nn, unsigned keep, cudaStream_t st);
 
 // Narrowing copies to FP32 (complex and real).
 cudaError_t to_f32_launch(const double2 *x, float2 *y, int64_t n, cudaStream_t st);

@@ -72,7 +72,8 @@ struct Solver {
     float2 *LV32 = nullptr, *LQ32 = nullptr;  // the same in complex64 (unused by the mixed s-step solve)
     float2 *Z32 = nullptr;  // mixed inner solve: the power basis Z_0..Z_order (complex64)
     bool mixed = false;
-    double exch_sign = 0.0;  // +1 / -1: exchange symmetry of the start block (mixed form), 0: none
+    double exch_sign = 0.0;     // +1 / -1: exchange symmetry of the start block, 0: none
+    unsigned refl_keep = 0xFFu;  // reflection sectors the start block reaches (bit c: sector c)
     // The mixed form's self-check: complex64 rounding amplified by the
     // conditioning of the k x k Gram (G^-1/2); a gross-failure detector.
     static constexpr double kOrthoTolMixed = 1e-3;
@@ -887,49 +888,81 @@ struct Solver {
         } else if (mixed) {
             s = equilibrate(b, k);
             if (s == DE_OK) s = basic_sstep(b, k);
-            // FP32 rounding in the inner solve breaks the electron-exchange
-            // symmetry that H and the FP64 iteration keep exactly; the
-            // contamination would stall the residual near 1e-6.  Restore it.
-            for (int j = 0; s == DE_OK && exch_sign != 0.0 && j < k; ++j) {
-                cudaError_t e = exch_project_launch(col(b, j), h->m, exch_sign, st);
-                if (e != cudaSuccess) s = cuda_error(e, "exch_project");
-            }
+            // Complex64 rounding in the inner solve leaks ~1e-7 into the
+            // exchange and reflection sectors that H and the FP64 iteration
+            // keep exactly, and the outer iteration then amplifies a leaked
+            // state lying nearer sigma: triplet solves stalled near 1e-6 on
+            // singlet contamination, and at N = 4 a state of one reflection
+            // class stalled near 3e-8 while a state of another class, nearer
+            // sigma, grew in.  Project back onto the start block's sectors.
+            if (s == DE_OK) s = symmetry_project(b, k);
         } else {
             s = equilibrate(b, k);
             if (s == DE_OK) s = basic<double2>(b, k);
-            // Block solves (NEV > 1) keep the start block's exchange sector
-            // too: in exact arithmetic the iteration never leaves it, but
-            // FP64 rounding leaks into the other sector, and GPLMR then
-            // converges to whichever sector's states lie nearest sigma (at
-            // N = 3, 4 with NEV = 4 a singlet start found a triplet triple).
-            for (int j = 0; s == DE_OK && k > 1 && exch_sign != 0.0 && j < k; ++j) {
-                cudaError_t e = exch_project_launch(col(b, j), h->m, exch_sign, st);
-                if (e != cudaSuccess) s = cuda_error(e, "exch_project");
-            }
+            // Block solves (NEV > 1) keep the start block's sectors too: in
+            // exact arithmetic the iteration never leaves them, but FP64
+            // rounding leaks into the others, and GPLMR then converges to
+            // whichever sector's states lie nearest sigma (at N = 3, 4 with
+            // NEV = 4 a singlet start found a triplet triple).
+            if (s == DE_OK && k > 1) s = symmetry_project(b, k);
         }
         t_prec += secs(t0, clk::now());
         return s;
     }
 
-    // Exchange symmetry of the (normalised) start block: every column
-    // symmetric (singlet, <x, x^T> = 1) or every column antisymmetric
-    // (triplet, -1) to 1e-8; anything else leaves the projection off.
-    int detect_exchange_symmetry()
+    // Symmetries of the (normalised) start block that the iteration keeps.
+    // Exchange: every column symmetric (singlet, <x, x^T> = 1) or every
+    // column antisymmetric (triplet, -1) to 1e-8; anything else leaves that
+    // projection off.  Reflections: H commutes with the three axis
+    // reflections c -> nn-1-c (both electrons at once), whose 8 characters
+    // split the space into sectors; a sector counts as reached when some
+    // column's component there has a squared norm above 1e-12 of the
+    // column's (the rounding of a start built in FP64 puts ~1e-30 into the
+    // others).  A start that reaches all 8 (a random one) leaves the
+    // projection off.
+    int detect_symmetry()
     {
         double sign = 0.0;
         for (int j = 0; j < nev; ++j) {
             cudaError_t e = exch_dot_launch(col(X, j), h->m, dR + j, h->d_work, st);
             if (e != cudaSuccess) return cuda_error(e, "exch_dot");
+            e = refl_corr_launch(col(X, j), h->nn, dG + 8 * j, h->d_work, st);
+            if (e != cudaSuccess) return cuda_error(e, "refl_corr");
         }
         DE_CUDA(cudaMemcpyAsync(hbuf, dR, nev * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        DE_CUDA(cudaMemcpyAsync(hbuf + nev, dG, 8 * nev * sizeof(double2), cudaMemcpyDeviceToHost, st));
         DE_CUDA(cudaStreamSynchronize(st));
+        unsigned keep = 0;
         for (int j = 0; j < nev; ++j) {
             const double r = hbuf[j].x;
             const double sj = std::fabs(r - 1.0) < 1e-8 ? 1.0 : std::fabs(r + 1.0) < 1e-8 ? -1.0 : 0.0;
             if (j == 0) sign = sj;
             else if (sj != sign) sign = 0.0;
+            const double2 *corr = hbuf + nev + 8 * j;  // <x, R_r x>, r = 0..7; r = 0 is |x|^2
+            for (int c = 0; c < 8; ++c) {
+                double n2 = 0.0;
+                for (int rr = 0; rr < 8; ++rr) n2 += ((__builtin_popcount(c & rr) & 1) ? -1.0 : 1.0) * corr[rr].x;
+                if (n2 / 8.0 > 1e-12 * corr[0].x) keep |= 1u << c;
+            }
         }
         exch_sign = sign;
+        refl_keep = keep;
+        return DE_OK;
+    }
+
+    // Projection of k preconditioned columns onto the start block's sectors.
+    int symmetry_project(double2 *b, int k)
+    {
+        for (int j = 0; j < k; ++j) {
+            if (exch_sign != 0.0) {
+                cudaError_t e = exch_project_launch(col(b, j), h->m, exch_sign, st);
+                if (e != cudaSuccess) return cuda_error(e, "exch_project");
+            }
+            if (refl_keep != 0xFFu) {
+                cudaError_t e = refl_project_launch(col(b, j), h->nn, refl_keep, st);
+                if (e != cudaSuccess) return cuda_error(e, "refl_project");
+            }
+        }
         return DE_OK;
     }
 
@@ -941,7 +974,7 @@ struct Solver {
         DE_TRY(setup());
         DE_TRY(normalize(X, nev));
         if ((mixed || (nev > 1 && !compat)) && order > 1 && gm.usepetscflag != 0)
-            DE_TRY(detect_exchange_symmetry());
+            DE_TRY(detect_symmetry());
         DE_TRY(matblock(X, AX, nev));
         std::vector<cplx> E;
         std::vector<double> res;

@@ -145,6 +145,8 @@ EV_SHAPE(double, 9, 0, 2, 2, 1, 1, 0)
 EV_SHAPE(double, 9, 1, 1, 5, 1, 2, 0)
 EV_SHAPE(double, 11, 0, 2, 2, 1, 1, 0)
 EV_SHAPE(double, 11, 1, 1, 3, 1, 2, 0)
+EV_SHAPE(double, 13, 0, 1, 4, 1, 1, 0)
+EV_SHAPE(double, 13, 1, 1, 4, 1, 1, 0)
 #undef EV_SHAPE
 
 template <class R, int NN, int MODE>
@@ -658,7 +660,7 @@ cudaError_t ev_dispatch(const HamDev &h, const CX<R> *x, CX<R> *y, int nvec, int
 {
 #define EV_CASE(NNV)                                                                       \
     case NNV:                                                                              \
-        if constexpr (NNV > (sizeof(R) == 8 ? 11 : 17)) return cudaErrorInvalidValue;      \
+        if constexpr (NNV > (sizeof(R) == 8 ? 13 : 17)) return cudaErrorInvalidValue;      \
         else                                                                               \
             return pass == 0 ? ev_launch<R, NNV, 0>(h, x, y, nvec, vstride, shs, st)       \
                              : ev_launch<R, NNV, 1>(h, x, y, nvec, vstride, shs, st);
@@ -680,8 +682,8 @@ cudaError_t ev_dispatch(const HamDev &h, const CX<R> *x, CX<R> *y, int nvec, int
 }  // namespace
 
 // Grids where these kernels beat the streaming / cube kernels on B200 (block
-// matvec timings at N = 4..10): complex64 NN = 9..17, complex128 NN = 9, 11.
-bool hammult_ev_supported(int nn, bool fp64) { return nn >= 9 && nn <= (fp64 ? 11 : 17); }
+// matvec timings at N = 4..10): complex64 NN = 9..17, complex128 NN = 9..13.
+bool hammult_ev_supported(int nn, bool fp64) { return nn >= 9 && nn <= (fp64 ? 13 : 17); }
 
 cudaError_t hammult_ev_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,
                                    int pass, cudaStream_t st, double2 shs)

@@ -148,7 +148,7 @@ DE_API int de_set_profiling(de_problem *h, int on);
 /* Which matvec kernels a handle uses: DE_MATVEC_FMA (the default) the
  * fastest CUDA-core kernels per grid: even/odd-split contractions for the
  * mixed form's complex64 matvec at NN = 9..17 and the plain form's at NN =
- * 9, 11, streaming kernels at NN = 13..19 otherwise, shared-memory cube
+ * 9..13, streaming kernels at NN = 15..19 otherwise, shared-memory cube
  * kernels elsewhere; DE_MATVEC_TENSOR the axis contractions on the FP64
  * tensor cores (DMMA) for NN = 9..19; DE_MATVEC_STREAM the streaming / cube
  * kernels everywhere (for comparison).  All give the reference's H x to

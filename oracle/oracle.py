@@ -369,6 +369,53 @@ def basicblocklansolve(x: np.ndarray, order: int, maxiter: int, sigma: complex, 
     return vf[:, :thisdim] @ solve
 
 
+def _refl_image(v: np.ndarray, nn: int, r: int) -> np.ndarray:
+    """R_r v: the axis reflections c -> nn-1-c of every axis a with bit a of
+    r set, applied to both electrons (v flat, x1 fastest)."""
+    a = v.reshape((nn,) * 6)  # C order: z2, y2, x2, z1, y1, x1
+    for ax in range(3):
+        if (r >> ax) & 1:
+            a = np.flip(np.flip(a, 5 - ax), 2 - ax)
+    return a.reshape(-1)
+
+
+def reflection_sectors(x: np.ndarray, nn: int, rel: float = 1e-12) -> int:
+    """Bit mask of the reflection sectors the columns of x reach: sector c
+    (0..7) is the eigenspace where R_r has eigenvalue (-1)^popcount(c & r);
+    a column reaches it when its component there has a squared norm above
+    rel of the column's.  The library keeps the preconditioned blocks of
+    its mixed form and of FP64 block solves in these sectors."""
+    keep = 0
+    for j in range(x.shape[1]):
+        v = x[:, j]
+        corr = [np.vdot(v, _refl_image(v, nn, r)).real for r in range(8)]
+        for c in range(8):
+            n2 = sum((-1) ** bin(c & r).count("1") * corr[r] for r in range(8)) / 8
+            if n2 > rel * corr[0]:
+                keep |= 1 << c
+    return keep
+
+
+def _round_c64(z: np.ndarray) -> np.ndarray:
+    """Complex64 storage of a complex128 block (the mixed form's power basis)."""
+    return z.astype(np.complex64).astype(np.complex128)
+
+
+def reflection_project(v: np.ndarray, nn: int, keep: int) -> np.ndarray:
+    """Projection of one flat vector onto the reflection sectors in keep:
+    sum over kept c of (1/8) sum_r (-1)^popcount(c & r) R_r v."""
+    w = np.zeros(8)
+    for c in range(8):
+        if (keep >> c) & 1:
+            for r in range(8):
+                w[r] += (-1) ** bin(c & r).count("1")
+    out = np.zeros_like(v)
+    for r in range(8):
+        if w[r] != 0.0:
+            out += (w[r] / 8) * _refl_image(v, nn, r)
+    return out
+
+
 def sstep_minres(x: np.ndarray, order: int, sigma: complex, mult, store=None) -> np.ndarray:
     """The library's mixed-form inner solve: the same minimal-residual
     approximation of (H - sigma)^{-1} X over the block Krylov space
@@ -524,7 +571,7 @@ def gplmr_eig(h: Hamiltonian, x0: np.ndarray, sigma: complex, ns: int = 5, maxit
               tol: float = 1e-7, order: int = 5, compat_first_column_only: bool = False,
               max_inner_iter: int | None = None, verbose: bool = False, usepetscflag: int = 1,
               gm_tol: float = 1e-3, gm_shift: complex = 0.0, equilibrate: bool = True,
-              exchange_project: bool = True) -> GplmrResult:
+              symmetry_project: bool = True, mixed: bool = False) -> GplmrResult:
     """GPLMR_EIG gplmr.F90:9-374 with the BASIC preconditioner, or with
     usepetscflag = 0 the PETSc GMRES one (PRECBLOCK gplmr.F90:466-502):
     GMRES on (H - gm_shift) per column with rtol gm_tol.  The reference's
@@ -543,12 +590,22 @@ def gplmr_eig(h: Hamiltonian, x0: np.ndarray, sigma: complex, ns: int = 5, maxit
     GPLMR's next step, cholQR, removes the scale, so the iteration is the
     same in exact arithmetic.  The first-column-only mode is never scaled.
 
-    exchange_project (default on; off restates the reference): a block
+    symmetry_project (default on; off restates the reference): a block
     solve (NEV > 1, BASIC path) whose start columns are all exchange-
     symmetric (or all antisymmetric) projects each preconditioned block back
-    onto that sector, X <- (X +- X^T)/2.  Exact arithmetic never leaves the
-    sector; rounding does, and at N = 3, 4 with NEV = 4 a singlet start
-    otherwise converges to a triplet triple nearer sigma."""
+    onto that sector, X <- (X +- X^T)/2, and onto the reflection sectors
+    the start columns reach (reflection_sectors; a no-op for a start that
+    reaches all eight).  Exact arithmetic never leaves these sectors;
+    rounding does, and at N = 3, 4 with NEV = 4 a singlet start otherwise
+    converges to a triplet triple nearer sigma.
+
+    mixed: the library's mixed form.  The inner solve is sstep_minres with
+    its power basis rounded to complex64 (the library's FP32 matvecs are
+    emulated by rounding FP64 ones), and every preconditioned block, for
+    any NEV, is projected back onto the start block's exchange sector and
+    onto the reflection sectors its columns reach: complex64 rounding leaks
+    into the other sectors at the 1e-7 level, and the iteration amplifies a
+    leaked state that lies nearer sigma."""
     if max_inner_iter is None:
         max_inner_iter = order
     calls0 = h.calls
@@ -574,24 +631,39 @@ def gplmr_eig(h: Hamiltonian, x0: np.ndarray, sigma: complex, ns: int = 5, maxit
                 return out
             return h.matblock(v)
 
+        if mixed:
+            blk = blk / colnorms(blk)[None, :]
+            out = sstep_minres(blk, max_inner_iter, sigma, mult, store=_round_c64)
+            return project(out)
         if equilibrate and not compat_first_column_only and blk.shape[1] > 1:
             # unit columns: the inner solve's output is linear in column
             # scaling and cholQR removes it again, so only the conditioning
             # of harm_orthog_oneblock's Gram changes (see gplmr_eig)
             blk = blk / colnorms(blk)[None, :]
         out = basicblocklansolve(blk, max_inner_iter, h.params.m ** 2, sigma, mult)
-        if exch_sign != 0.0 and blk.shape[1] > 1:
-            m = h.params.m
-            for j in range(out.shape[1]):
+        return project(out) if blk.shape[1] > 1 else out
+
+    def project(out: np.ndarray) -> np.ndarray:
+        m = h.params.m
+        for j in range(out.shape[1]):
+            if exch_sign != 0.0:
                 z = out[:, j].reshape(m, m, order="F")
                 out[:, j] = (0.5 * (z + exch_sign * z.T)).reshape(-1, order="F")
+            if refl_keep != 0xFF:
+                out[:, j] = reflection_project(out[:, j], h.params.nn, refl_keep)
         return out
 
     x /= colnorms(x)[None, :]
     # exchange sector of the start block (+1 every column symmetric, -1
-    # every column antisymmetric, 0 otherwise), kept by block solves
+    # every column antisymmetric, 0 otherwise) and the reflection sectors its
+    # columns reach, kept by block solves and by the mixed form
     exch_sign = 0.0
-    if exchange_project and nev > 1 and not compat_first_column_only and usepetscflag != 0 and max_inner_iter > 1:
+    refl_keep = 0xFF
+    if mixed and (compat_first_column_only or usepetscflag == 0 or max_inner_iter < 2):
+        raise ValueError("the mixed form is the BASIC inner solve of order >= 2")
+    if (mixed or (symmetry_project and nev > 1)) and not compat_first_column_only and usepetscflag != 0 \
+            and max_inner_iter > 1:
+        refl_keep = reflection_sectors(x, h.params.nn)
         m = h.params.m
         signs = []
         for j in range(nev):

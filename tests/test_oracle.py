@@ -294,3 +294,28 @@ def test_power_basis_inner_solve_equals_basicblocklansolve():
         ref = O.basicblocklansolve(x, 5, p.m ** 2, complex(-0.78, 0.0), h.matblock)
         got = O.sstep_minres(x, 5, complex(-0.78, 0.0), h.matblock)
         assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-8
+
+
+def test_reflection_sectors_are_symmetries_of_h():
+    """The axis reflections c -> nn-1-c (both electrons at once) commute with
+    H, so the sector projections do too; each projection is idempotent, the
+    eight of them sum to the identity, and a vector projected onto some
+    sectors reaches only those."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    p = O.Params(n=2, delta=2.0, theta=0.3)
+    h = O.init_hamiltonian(p, nelec=2)
+    x = O.seeded_start(p, 1, 5)[:, 0]
+    total = np.zeros_like(x)
+    for c in range(8):
+        px = O.reflection_project(x, p.nn, 1 << c)
+        assert np.linalg.norm(O.reflection_project(px, p.nn, 1 << c) - px) < 1e-13 * np.linalg.norm(x)
+        hp = h.matvec(px)
+        assert np.linalg.norm(hp - O.reflection_project(hp, p.nn, 1 << c)) < 1e-12 * np.linalg.norm(hp)
+        total += px
+    assert np.linalg.norm(total - x) < 1e-13 * np.linalg.norm(x)
+    assert O.reflection_sectors(x[:, None], p.nn) == 0xFF
+    y = O.reflection_project(x, p.nn, 0x68)
+    assert O.reflection_sectors(y[:, None], p.nn) == 0x68
