@@ -103,8 +103,10 @@ class Problem:
         """'fma' (default): the CUDA-core kernels on even/odd-split
         contractions; 'tensor': the axis contractions on the FP64 tensor
         cores where built (NN 9..19); 'stream': the earlier CUDA-core
-        streaming kernels (NN 13..19)."""
-        kinds = {"fma": 0, "tensor": 1, "stream": 2}
+        streaming kernels (NN 13..19); 'tf32': the complex64 matvec's
+        kinetic contractions on the TF32 tensor cores with head/tail split
+        operands (NN 9..15)."""
+        kinds = {"fma": 0, "tensor": 1, "stream": 2, "tf32": 3}
         if kind not in kinds:
             raise ValueError(f"matvec kernel must be one of {sorted(kinds)}")
         check(lib().de_set_matvec_kernel(self._h, kinds[kind]), "de_set_matvec_kernel")

@@ -400,9 +400,11 @@ DE_API int de_set_stream(de_problem *h, void *s)
 DE_API int de_set_matvec_kernel(de_problem *h, int kind)
 {
     if (!h) return set_error(DE_E_INVALID, "null handle");
-    if (kind != DE_MATVEC_FMA && kind != DE_MATVEC_TENSOR && kind != DE_MATVEC_STREAM)
+    if (kind != DE_MATVEC_FMA && kind != DE_MATVEC_TENSOR && kind != DE_MATVEC_STREAM && kind != DE_MATVEC_TF32)
         return set_error(DE_E_INVALID,
-                         "matvec kernel must be DE_MATVEC_FMA, DE_MATVEC_TENSOR or DE_MATVEC_STREAM (got %d)", kind);
+                         "matvec kernel must be DE_MATVEC_FMA, DE_MATVEC_TENSOR, DE_MATVEC_STREAM or DE_MATVEC_TF32 "
+                         "(got %d)",
+                         kind);
     std::lock_guard<std::mutex> lk(h->mu);
     h->ham.tc = kind;
     return DE_OK;

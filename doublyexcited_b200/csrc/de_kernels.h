@@ -32,7 +32,8 @@ struct HamDev {
     const float *t1af;
     const float *v12f;
     int tc;  // matvec kernels: 0 even/odd (hammult_ev.cu), 1 FP64 tensor cores (hammult_tc.cu),
-             // 2 the earlier streaming kernels (hammult.cu)
+             // 2 the earlier streaming kernels (hammult.cu), 3 the complex64 passes on the
+             // TF32 tensor cores (hammult_tc32.cu; complex128 passes as 0)
     // Even/odd-split coefficients of T for the grid (hammult_ev.cu), index
     // a * (N+1) + b: ev_ce(a,0) = t(a), ev_ce(a,b) = (t(|a-b|) + t(a+b))/2,
     // ev_co(a,b) = (t(|a-b|) - t(a+b))/2 (a, b >= 1); FP32 copies beside.
@@ -62,6 +63,17 @@ cudaError_t hammult_pass_launch(const HamDev &h, const float2 *x, float2 *y, int
 // hammult_ev_supported accepts (complex128: NN = 9..13; complex64: NN =
 // 9..17); shs is the diagonal shift times SCALE^2.
 bool hammult_ev_supported(int nn, bool fp64);
+
+// The complex64 passes with the kinetic contractions on the tensor cores
+// (tcgen05 kind::tf32, head/tail split; hammult_tc32.cu) for the grids
+// hammult_tc32_supported accepts (NN = 9..15); shs as above.  The kernels
+// record a timed-out mbarrier wait in a device flag that
+// hammult_tc32_error reads and clears (1 = a wait gave up, -1 = the read
+// failed).
+bool hammult_tc32_supported(int nn);
+cudaError_t hammult_tc32_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride,
+                                     int pass, cudaStream_t st, double2 shs);
+int hammult_tc32_error(cudaStream_t st);
 cudaError_t hammult_ev_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,
                                    int pass, cudaStream_t st, double2 shs);
 cudaError_t hammult_ev_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride, int pass,

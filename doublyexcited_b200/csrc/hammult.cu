@@ -662,8 +662,12 @@ static cudaError_t pass_go(const HamDev &h, const C2<R> *x, C2<R> *y, int nvec, 
     if (sizeof(R) == 4 && (!h.t1af || !h.v12f)) return cudaErrorInvalidValue;
     if (h.tc == 1 && hammult_tc_supported(h.nn)) return hammult_tc_pass_launch(h, x, y, nvec, vstride, pass, st, shift);
     const CubeArgs<R> a = make_args<R>(h, x, y, vstride, shift);
+    if constexpr (sizeof(R) == 4) {
+        if (h.tc == 3 && hammult_tc32_supported(h.nn))
+            return hammult_tc32_pass_launch(h, x, y, nvec, vstride, pass, st, a.shs);
+    }
     // even/odd kernels where they are the faster ones (hammult_ev_supported)
-    if (h.tc == 0 && hammult_ev_supported(h.nn, sizeof(R) == 8))
+    if ((h.tc == 0 || h.tc == 3) && hammult_ev_supported(h.nn, sizeof(R) == 8))
         return hammult_ev_pass_launch(h, x, y, nvec, vstride, pass, st, a.shs);
     const int64_t ncubes = h.m * (int64_t)nvec;
     if (ncubes > 0x7fffffffLL) return cudaErrorInvalidValue;

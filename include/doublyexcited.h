@@ -151,9 +151,12 @@ DE_API int de_set_profiling(de_problem *h, int on);
  * 9..13, streaming kernels at NN = 15..19 otherwise, shared-memory cube
  * kernels elsewhere; DE_MATVEC_TENSOR the axis contractions on the FP64
  * tensor cores (DMMA) for NN = 9..19; DE_MATVEC_STREAM the streaming / cube
- * kernels everywhere (for comparison).  All give the reference's H x to
- * rounding. */
-enum { DE_MATVEC_FMA = 0, DE_MATVEC_TENSOR = 1, DE_MATVEC_STREAM = 2 };
+ * kernels everywhere (for comparison); DE_MATVEC_TF32 the mixed form's
+ * complex64 matvec with its kinetic contractions on the 5th-generation
+ * tensor cores (tcgen05, TF32 products of head/tail-split operands, FP32
+ * accuracy) for NN = 9..15, the FMA kernels elsewhere and for complex128.
+ * All give the reference's H x to rounding. */
+enum { DE_MATVEC_FMA = 0, DE_MATVEC_TENSOR = 1, DE_MATVEC_STREAM = 2, DE_MATVEC_TF32 = 3 };
 DE_API int de_set_matvec_kernel(de_problem *h, int kind);
 /* Device milliseconds of pass A and pass B, MATBLOCK calls and vectors
  * multiplied since the last read (waits for the recorded events); resets. */

@@ -17,6 +17,8 @@ def _run(de, oracle, g, **kw):
     op = oracle.Params(n=p["n"], delta=p["delta"], theta=p["theta"])
     x0 = oracle.seeded_start(op, st["nev"], st["seed"], st["spin"])
     with de.Problem(n=p["n"], delta=p["delta"], theta=p["theta"], precision=kw.get("precision", "fp64")) as h:
+        if "kernel" in kw:
+            h.set_matvec_kernel(kw["kernel"])
         return h.gplmr_eig(x0, complex(*s["sigma"]), ns=s["ns"], maxit=kw.get("maxit", s["maxit"]),
                            tol=s["tol"], max_inner_iter=s["order"],
                            compat_first_column_only=s["compat_first_column_only"])
@@ -134,6 +136,17 @@ def test_gplmr_mixed_precision_resonance(de, oracle, name):
     the iterates but not the converged eigenvalue."""
     g = load_json(name)
     r = _run(de, oracle, g, precision="mixed")
+    assert r.converged and r.max_residual <= g["solver"]["tol"]
+    assert abs(r.e[0] - complex(*g["e"][0])) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["gplmr_n5_nev1.json", "gplmr_n6_nev1.json"])
+def test_mixed_solve_on_tf32_tensor_cores(de, oracle, name):
+    """The mixed form with its complex64 matvecs on the TF32 tensor cores
+    (tcgen05, head/tail-split operands): the same resonance as the oracle's
+    FP64 run within 1e-9 Hartree."""
+    g = load_json(name)
+    r = _run(de, oracle, g, precision="mixed", kernel="tf32")
     assert r.converged and r.max_residual <= g["solver"]["tol"]
     assert abs(r.e[0] - complex(*g["e"][0])) < 1e-9
 

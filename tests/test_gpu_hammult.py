@@ -126,7 +126,7 @@ def test_device_pointer_api(de, oracle):
     assert np.array_equal(y, ref)
 
 
-@pytest.mark.parametrize("kind", ["fma", "tensor"])
+@pytest.mark.parametrize("kind", ["fma", "tensor", "tf32"])
 @pytest.mark.parametrize("n,theta", [(3, 0.2), (5, 0.35), (6, 0.2)])
 def test_fp32_matvec_relative_error(de, oracle, n, theta, kind):
     """The mixed form's FP32 matvec on complex64 inputs, per call, against
@@ -268,3 +268,31 @@ def test_even_odd_kernels_match_streaming_kernels(de, n):
         ref = ys["stream"][0][j]
         assert (torch.linalg.norm(ys["fma"][0][j] - ref) / torch.linalg.norm(ref)).item() < 1e-13
         assert (torch.linalg.norm(ys["fma"][1][j] - ref) / torch.linalg.norm(ref)).item() < 1e-6
+
+
+@pytest.mark.parametrize("n", [4, 5, 6, 7])
+def test_tf32_tensor_core_matvec(de, n):
+    """The complex64 matvec with its kinetic contractions on the TF32 tensor
+    cores (tcgen05, head/tail-split operands) against the FP64 matvec, on a
+    block of two vectors: within 1e-6 relative, the FP32 bar; N=4..7 are the
+    grids it serves (NN 9..15), both passes' partial last batches
+    included."""
+    import torch
+
+    with de.Problem(n=n, delta=2.0, theta=0.3) as g64, \
+            de.Problem(n=n, delta=2.0, theta=0.3, precision="mixed") as g32:
+        st = torch.cuda.current_stream()
+        g64.set_stream(st.cuda_stream)
+        g32.set_stream(st.cuda_stream)
+        gen = torch.Generator(device="cuda").manual_seed(70 + n)
+        x = torch.randn(2, g64.dim, dtype=torch.complex128, device="cuda", generator=gen)
+        y = torch.empty_like(x)
+        g64.matblock_d(x.data_ptr(), y.data_ptr(), 2)
+        g32.set_matvec_kernel("tf32")
+        x32 = x.to(torch.complex64)
+        y32 = torch.empty_like(x32)
+        g32.matblock32_d(x32.data_ptr(), y32.data_ptr(), 2)
+        torch.cuda.synchronize()
+    for j in range(2):
+        err = (torch.linalg.norm(y32[j].to(torch.complex128) - y[j]) / torch.linalg.norm(y[j])).item()
+        assert err < 1e-6, err
