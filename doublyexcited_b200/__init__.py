@@ -21,6 +21,9 @@ mirroring the reference's entry points (paths relative to
 * :func:`write_vectors` / :func:`read_vectors` -- utils.F90:82-198
 * :class:`Server` -- many independent solves on one GPU (no reference
   counterpart): admission by device footprint, concurrent streams
+* ``python -m doublyexcited_b200.tune`` -- the matvec autotuner: times each
+  kernel family and resident-CTA count per grid and pass on the GPU and
+  writes the table the library reads (:func:`tuning_lookup`)
 
 There is no CPU fallback: if the library is missing or no GPU is present the
 calls raise.
@@ -46,7 +49,7 @@ from ._lib import (  # noqa: F401
     lib,
     lib_path,
 )
-from .api import Problem, GplmrResult, RunResult, Server, ServedResult, heplus_orbitals, read_input, read_vectors, run, vectors_header, write_vectors  # noqa: F401,E501
+from .api import Problem, GplmrResult, RunResult, Server, ServedResult, heplus_orbitals, read_input, read_vectors, run, tuning_lookup, vectors_header, write_vectors  # noqa: F401,E501
 
 __all__ = [
     "Problem",
@@ -60,6 +63,7 @@ __all__ = [
     "read_vectors",
     "vectors_header",
     "write_vectors",
+    "tuning_lookup",
     "DeError",
     "lib",
     "lib_path",

@@ -198,6 +198,9 @@ SIGNATURES = {
     "de_server_destroy": (INT, [P]),
     "de_problem_trim": (INT, [P]),
     "de_set_matvec_kernel": (INT, [P, INT]),
+    "de_set_matvec_launch": (INT, [P, INT, INT, INT, INT]),
+    "de_get_matvec_launch": (INT, [P, INT, INT, P, P]),
+    "de_tuning_lookup": (INT, [ctypes.c_char_p, INT, INT, INT, P, P]),
 }
 
 _LIB = None

@@ -111,6 +111,23 @@ class Problem:
             raise ValueError(f"matvec kernel must be one of {sorted(kinds)}")
         check(lib().de_set_matvec_kernel(self._h, kinds[kind]), "de_set_matvec_kernel")
 
+    FAMILIES = ("fma", "tensor", "stream", "tf32")
+
+    def set_matvec_launch(self, storage: str, pass_: int, family: str, ctas_per_sm: int = 0) -> None:
+        """The kernels of one matvec pass: storage 'c128' (the FP64
+        matvecs) or 'c64' (the mixed form's inner solve), pass 0 (electron-2
+        axes and potential) or 1 (electron-1 axes), a family of
+        set_matvec_kernel and a cap on resident CTAs per SM (0: all)."""
+        check(lib().de_set_matvec_launch(self._h, {"c128": 0, "c64": 1}[storage], pass_,
+                                         self.FAMILIES.index(family), ctas_per_sm), "de_set_matvec_launch")
+
+    def get_matvec_launch(self, storage: str, pass_: int) -> tuple:
+        """(family, ctas_per_sm) of one pass (see set_matvec_launch)."""
+        f, c = ctypes.c_int(), ctypes.c_int()
+        check(lib().de_get_matvec_launch(self._h, {"c128": 0, "c64": 1}[storage], pass_, ctypes.byref(f),
+                                         ctypes.byref(c)), "de_get_matvec_launch")
+        return self.FAMILIES[f.value], c.value
+
     def set_profiling(self, on: bool) -> None:
         check(lib().de_set_profiling(self._h, int(bool(on))), "de_set_profiling")
 
@@ -425,3 +442,15 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def tuning_lookup(path: str, storage: str, nn: int, pass_: int) -> tuple | None:
+    """A tuning table's (family, ctas_per_sm) for storage 'c128'/'c64', grid
+    NN and pass 0/1, or None when the file or the entry is missing (host
+    only; see set_matvec_launch)."""
+    f, c = ctypes.c_int(), ctypes.c_int()
+    st = lib().de_tuning_lookup(path.encode(), {"c128": 0, "c64": 1}[storage], nn, pass_, ctypes.byref(f),
+                                ctypes.byref(c))
+    if st != 0:
+        return None
+    return Problem.FAMILIES[f.value], c.value

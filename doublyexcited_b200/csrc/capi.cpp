@@ -315,7 +315,7 @@ DE_API int de_problem_create(const de_params *pin, de_problem **out)
     hd.vsim = vs.imag();
     hd.sre = scale.real();
     hd.sim = scale.imag();
-    hd.tc = 0;  // the even/odd CUDA-core kernels (de_set_matvec_kernel)
+    apply_tuning(hd);  // kernel family and CTAs per SM of each pass (de_set_matvec_kernel overrides)
 
     auto tinv = cached_tinv(nbig_alloc, nbig_solve, p.nsmall, delta);
     const int nbd = 2 * nbig_alloc + 1;
@@ -406,7 +406,48 @@ DE_API int de_set_matvec_kernel(de_problem *h, int kind)
                          "(got %d)",
                          kind);
     std::lock_guard<std::mutex> lk(h->mu);
-    h->ham.tc = kind;
+    for (int s = 0; s < 2; ++s)
+        for (int p = 0; p < 2; ++p) {
+            // DE_MATVEC_TF32 is a complex64 form; complex128 passes keep the FMA kernels
+            h->ham.fam[s][p] = (signed char)(kind == DE_MATVEC_TF32 && s == 0 ? DE_MATVEC_FMA : kind);
+            h->ham.ctas[s][p] = 0;
+        }
+    return DE_OK;
+}
+
+DE_API int de_set_matvec_launch(de_problem *h, int storage, int pass, int family, int ctas_per_sm)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    if (storage < 0 || storage > 1 || pass < 0 || pass > 1)
+        return set_error(DE_E_INVALID, "storage must be 0 or 1 and pass 0 or 1 (got %d, %d)", storage, pass);
+    if (family < DE_MATVEC_FMA || family > DE_MATVEC_TF32 || ctas_per_sm < 0 || ctas_per_sm > 32)
+        return set_error(DE_E_INVALID, "family must be a DE_MATVEC_* kind and ctas_per_sm 0..32 (got %d, %d)", family,
+                         ctas_per_sm);
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->ham.fam[storage][pass] = (signed char)family;
+    h->ham.ctas[storage][pass] = (signed char)ctas_per_sm;
+    return DE_OK;
+}
+
+DE_API int de_get_matvec_launch(de_problem *h, int storage, int pass, int *family, int *ctas_per_sm)
+{
+    if (!h || !family || !ctas_per_sm) return set_error(DE_E_INVALID, "null argument");
+    if (storage < 0 || storage > 1 || pass < 0 || pass > 1)
+        return set_error(DE_E_INVALID, "storage must be 0 or 1 and pass 0 or 1 (got %d, %d)", storage, pass);
+    std::lock_guard<std::mutex> lk(h->mu);
+    *family = h->ham.fam[storage][pass];
+    *ctas_per_sm = h->ham.ctas[storage][pass];
+    return DE_OK;
+}
+
+DE_API int de_tuning_lookup(const char *path, int storage, int nn, int pass, int *family, int *ctas_per_sm)
+{
+    if (!path || !family || !ctas_per_sm) return set_error(DE_E_INVALID, "null argument");
+    int f = 0, c = 0;
+    if (!de::tuning_lookup(path, storage, nn, pass, f, c))
+        return set_error(DE_E_INVALID, "no tuning entry for storage %d, NN %d, pass %d in %s", storage, nn, pass, path);
+    *family = f;
+    *ctas_per_sm = c;
     return DE_OK;
 }
 

@@ -31,9 +31,15 @@ struct HamDev {
     float tf[kMaxNN];
     const float *t1af;
     const float *v12f;
-    int tc;  // matvec kernels: 0 even/odd (hammult_ev.cu), 1 FP64 tensor cores (hammult_tc.cu),
-             // 2 the earlier streaming kernels (hammult.cu), 3 the complex64 passes on the
-             // TF32 tensor cores (hammult_tc32.cu; complex128 passes as 0)
+    // Matvec kernels per [storage: 0 complex128, 1 complex64][pass: 0 A, 1 B]:
+    // fam 0 even/odd-split (hammult_ev.cu; streaming / cube where those are
+    // not built), 1 FP64 tensor cores (hammult_tc.cu), 2 streaming / cube
+    // (hammult.cu), 3 tcgen05 TF32 (hammult_tc32.cu, complex64 on NN 9..15;
+    // even/odd elsewhere); ctas = resident CTAs per SM of the persistent
+    // kernels, 0 = as many as fit.  Filled from the tuning table at creation
+    // (tuning.cpp) or by de_set_matvec_kernel / de_set_matvec_launch.
+    signed char fam[2][2];
+    signed char ctas[2][2];
     // Even/odd-split coefficients of T for the grid (hammult_ev.cu), index
     // a * (N+1) + b: ev_ce(a,0) = t(a), ev_ce(a,b) = (t(|a-b|) + t(a+b))/2,
     // ev_co(a,b) = (t(|a-b|) - t(a+b))/2 (a, b >= 1); FP32 copies beside.
@@ -43,6 +49,13 @@ struct HamDev {
 
 // Fills ev_ce / ev_co (and the FP32 copies) from h.t for grid h.nn.
 void fill_ev_coefficients(HamDev &h);
+
+// Tuning table (tuning.cpp): the entry of (storage 0 complex128 / 1
+// complex64, NN, pass) in the table at path; false when the file or the
+// entry is missing.  apply_tuning fills h.fam / h.ctas for h.nn from the
+// default table (built-in choices where it has no entry).
+bool tuning_lookup(const char *path, int storage, int nn, int pass, int &fam, int &ctas);
+void apply_tuning(HamDev &h);
 
 // Y(:,:,v) = H X(:,:,v) for v < nvec; vectors are vstride elements apart.
 // Two passes: electron-2 axes + potential (strided cubes, writes Y), then
@@ -72,12 +85,12 @@ bool hammult_ev_supported(int nn, bool fp64);
 // failed).
 bool hammult_tc32_supported(int nn);
 cudaError_t hammult_tc32_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride,
-                                     int pass, cudaStream_t st, double2 shs);
+                                     int pass, cudaStream_t st, double2 shs, int ctas = 0);
 int hammult_tc32_error(cudaStream_t st);
 cudaError_t hammult_ev_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,
-                                   int pass, cudaStream_t st, double2 shs);
+                                   int pass, cudaStream_t st, double2 shs, int ctas = 0);
 cudaError_t hammult_ev_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride, int pass,
-                                   cudaStream_t st, double2 shs);
+                                   cudaStream_t st, double2 shs, int ctas = 0);
 
 // Tensor-core (DMMA) form of one pass, for the grids hammult_tc_supported
 // accepts; the same arguments and results as hammult_pass_launch.

@@ -576,7 +576,7 @@ int sm_count()
 }
 
 template <class R, int NN, int MODE>
-cudaError_t launch_stream(const HamDev &h, const CubeArgs<R> &a, int64_t ncubes, cudaStream_t st)
+cudaError_t launch_stream(const HamDev &h, const CubeArgs<R> &a, int64_t ncubes, cudaStream_t st, int ctas)
 {
     using C = SCfg<NN, R>;
     const size_t smem = (size_t)4 * C::G * C::P2 * sizeof(C2<R>);
@@ -590,21 +590,22 @@ cudaError_t launch_stream(const HamDev &h, const CubeArgs<R> &a, int64_t ncubes,
         if (e != cudaSuccess) return e;
         attr[dev] = true;
     }
-    const int64_t grid = std::min<int64_t>(ncubes, (int64_t)sm_count() * smin_blocks<NN, R>());
+    const int per_sm = ctas > 0 ? std::min(ctas, smin_blocks<NN, R>()) : smin_blocks<NN, R>();
+    const int64_t grid = std::min<int64_t>(ncubes, (int64_t)sm_count() * per_sm);
     stream_kernel<R, NN, MODE><<<(unsigned)grid, C::NT, smem, st>>>(h, a, ncubes);
     count_launch();
     return cudaGetLastError();
 }
 
 template <class R, int MODE>
-cudaError_t dispatch(const HamDev &h, const CubeArgs<R> &a, int64_t ncubes, cudaStream_t st)
+cudaError_t dispatch(const HamDev &h, const CubeArgs<R> &a, int64_t ncubes, cudaStream_t st, int ctas = 0)
 {
     if constexpr (MODE != kOneElec) {
         switch (h.nn) {
-        case 13: return launch_stream<R, 13, MODE>(h, a, ncubes, st);
-        case 15: return launch_stream<R, 15, MODE>(h, a, ncubes, st);
-        case 17: return launch_stream<R, 17, MODE>(h, a, ncubes, st);
-        case 19: return launch_stream<R, 19, MODE>(h, a, ncubes, st);
+        case 13: return launch_stream<R, 13, MODE>(h, a, ncubes, st, ctas);
+        case 15: return launch_stream<R, 15, MODE>(h, a, ncubes, st, ctas);
+        case 17: return launch_stream<R, 17, MODE>(h, a, ncubes, st, ctas);
+        case 19: return launch_stream<R, 19, MODE>(h, a, ncubes, st, ctas);
         default: break;
         }
     }
@@ -660,18 +661,21 @@ static cudaError_t pass_go(const HamDev &h, const C2<R> *x, C2<R> *y, int nvec, 
 {
     if (h.nelec != 2 || nvec <= 0) return cudaErrorInvalidValue;
     if (sizeof(R) == 4 && (!h.t1af || !h.v12f)) return cudaErrorInvalidValue;
-    if (h.tc == 1 && hammult_tc_supported(h.nn)) return hammult_tc_pass_launch(h, x, y, nvec, vstride, pass, st, shift);
+    if (pass != 0 && pass != 1) return cudaErrorInvalidValue;
+    const int sto = sizeof(R) == 4 ? 1 : 0;
+    const int fam = h.fam[sto][pass], ctas = h.ctas[sto][pass];
+    if (fam == 1 && hammult_tc_supported(h.nn)) return hammult_tc_pass_launch(h, x, y, nvec, vstride, pass, st, shift);
     const CubeArgs<R> a = make_args<R>(h, x, y, vstride, shift);
     if constexpr (sizeof(R) == 4) {
-        if (h.tc == 3 && hammult_tc32_supported(h.nn))
-            return hammult_tc32_pass_launch(h, x, y, nvec, vstride, pass, st, a.shs);
+        if (fam == 3 && hammult_tc32_supported(h.nn))
+            return hammult_tc32_pass_launch(h, x, y, nvec, vstride, pass, st, a.shs, ctas);
     }
-    // even/odd kernels where they are the faster ones (hammult_ev_supported)
-    if ((h.tc == 0 || h.tc == 3) && hammult_ev_supported(h.nn, sizeof(R) == 8))
-        return hammult_ev_pass_launch(h, x, y, nvec, vstride, pass, st, a.shs);
+    // even/odd kernels where they are built (hammult_ev_supported)
+    if ((fam == 0 || fam == 1 || fam == 3) && hammult_ev_supported(h.nn, sizeof(R) == 8))
+        return hammult_ev_pass_launch(h, x, y, nvec, vstride, pass, st, a.shs, ctas);
     const int64_t ncubes = h.m * (int64_t)nvec;
     if (ncubes > 0x7fffffffLL) return cudaErrorInvalidValue;
-    return pass == 0 ? dispatch<R, kRowsPot>(h, a, ncubes, st) : dispatch<R, kColsAcc>(h, a, ncubes, st);
+    return pass == 0 ? dispatch<R, kRowsPot>(h, a, ncubes, st, ctas) : dispatch<R, kColsAcc>(h, a, ncubes, st, ctas);
 }
 
 cudaError_t hammult_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,

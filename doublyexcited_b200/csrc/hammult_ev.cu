@@ -635,12 +635,13 @@ cudaError_t ev_prepare(int &per_sm)
 
 template <class R, int NN, int MODE>
 cudaError_t ev_launch(const HamDev &h, const CX<R> *x, CX<R> *y, int nvec, int64_t vstride, double2 shs,
-                      cudaStream_t st)
+                      cudaStream_t st, int ctas)
 {
     using C = EvCfg<R, NN, MODE>;
     int per_sm = 1;
     cudaError_t e = ev_prepare<R, NN, MODE>(per_sm);
     if (e != cudaSuccess) return e;
+    if (ctas > 0) per_sm = std::min(per_sm, ctas);
     EvArgs<R> a{};
     a.x = x;
     a.y = y;
@@ -656,14 +657,14 @@ cudaError_t ev_launch(const HamDev &h, const CX<R> *x, CX<R> *y, int nvec, int64
 
 template <class R>
 cudaError_t ev_dispatch(const HamDev &h, const CX<R> *x, CX<R> *y, int nvec, int64_t vstride, int pass,
-                        double2 shs, cudaStream_t st)
+                        double2 shs, cudaStream_t st, int ctas)
 {
 #define EV_CASE(NNV)                                                                       \
     case NNV:                                                                              \
         if constexpr (NNV > (sizeof(R) == 8 ? 13 : 17)) return cudaErrorInvalidValue;      \
         else                                                                               \
-            return pass == 0 ? ev_launch<R, NNV, 0>(h, x, y, nvec, vstride, shs, st)       \
-                             : ev_launch<R, NNV, 1>(h, x, y, nvec, vstride, shs, st);
+            return pass == 0 ? ev_launch<R, NNV, 0>(h, x, y, nvec, vstride, shs, st, ctas) \
+                             : ev_launch<R, NNV, 1>(h, x, y, nvec, vstride, shs, st, ctas);
     switch (h.nn) {
 #ifdef EV_ONLY_NN
         EV_CASE(EV_ONLY_NN)
@@ -686,15 +687,15 @@ cudaError_t ev_dispatch(const HamDev &h, const CX<R> *x, CX<R> *y, int nvec, int
 bool hammult_ev_supported(int nn, bool fp64) { return nn >= 9 && nn <= (fp64 ? 13 : 17); }
 
 cudaError_t hammult_ev_pass_launch(const HamDev &h, const double2 *x, double2 *y, int nvec, int64_t vstride,
-                                   int pass, cudaStream_t st, double2 shs)
+                                   int pass, cudaStream_t st, double2 shs, int ctas)
 {
-    return ev_dispatch<double>(h, x, y, nvec, vstride, pass, shs, st);
+    return ev_dispatch<double>(h, x, y, nvec, vstride, pass, shs, st, ctas);
 }
 
 cudaError_t hammult_ev_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride, int pass,
-                                   cudaStream_t st, double2 shs)
+                                   cudaStream_t st, double2 shs, int ctas)
 {
-    return ev_dispatch<float>(h, x, y, nvec, vstride, pass, shs, st);
+    return ev_dispatch<float>(h, x, y, nvec, vstride, pass, shs, st, ctas);
 }
 
 }  // namespace de

@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(TcCfg<NN>::NT, 2) tc32_kernel(const __grid_con
     float2 *ys = reinterpret_cast<float2 *>(smem + C::Y_OFF);
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + C::BAR_OFF);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(smem + C::BAR_OFF + 8);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t sbase = smem_u32(smem), bar_s = smem_u32(bar);
 
     // T^T as the B operand, head and tail: row o (N), column k (K)
@@ -421,7 +421,7 @@ int tc32_sm_count()
 
 template <int NN, int MODE>
 cudaError_t tc32_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride, double2 shs,
-                        cudaStream_t st)
+                        cudaStream_t st, int ctas)
 {
     using C = TcCfg<NN>;
     static std::atomic<int> attr_done[64] = {};
@@ -440,7 +440,8 @@ cudaError_t tc32_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, i
     a.shs = shs;
     a.upv = (C::M + C::PB - 1) / C::PB;
     a.nunits = (int64_t)a.upv * nvec;
-    const int64_t grid = std::min<int64_t>(a.nunits, 2 * (int64_t)tc32_sm_count());
+    const int per_sm = ctas == 1 ? 1 : 2;  // two fit (launch bounds, shared memory)
+    const int64_t grid = std::min<int64_t>(a.nunits, per_sm * (int64_t)tc32_sm_count());
     tc32_kernel<NN, MODE><<<(unsigned)grid, C::NT, C::SMEM, st>>>(h, a);
     count_launch();
     return cudaGetLastError();
@@ -451,16 +452,21 @@ cudaError_t tc32_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, i
 bool hammult_tc32_supported(int nn) { return nn == 9 || nn == 11 || nn == 13 || nn == 15; }
 
 cudaError_t hammult_tc32_pass_launch(const HamDev &h, const float2 *x, float2 *y, int nvec, int64_t vstride,
-                                     int pass, cudaStream_t st, double2 shs)
+                                     int pass, cudaStream_t st, double2 shs, int ctas)
 {
     if (!h.t1af || !h.v12f) return cudaErrorInvalidValue;
+#define TC32_CASE(NNV)                                                        \
+    case NNV:                                                                 \
+        return pass == 0 ? tc32_launch<NNV, 0>(h, x, y, nvec, vstride, shs, st, ctas) \
+                         : tc32_launch<NNV, 1>(h, x, y, nvec, vstride, shs, st, ctas);
     switch (h.nn) {
-    case 9: return pass == 0 ? tc32_launch<9, 0>(h, x, y, nvec, vstride, shs, st) : tc32_launch<9, 1>(h, x, y, nvec, vstride, shs, st);
-    case 11: return pass == 0 ? tc32_launch<11, 0>(h, x, y, nvec, vstride, shs, st) : tc32_launch<11, 1>(h, x, y, nvec, vstride, shs, st);
-    case 13: return pass == 0 ? tc32_launch<13, 0>(h, x, y, nvec, vstride, shs, st) : tc32_launch<13, 1>(h, x, y, nvec, vstride, shs, st);
-    case 15: return pass == 0 ? tc32_launch<15, 0>(h, x, y, nvec, vstride, shs, st) : tc32_launch<15, 1>(h, x, y, nvec, vstride, shs, st);
+        TC32_CASE(9)
+        TC32_CASE(11)
+        TC32_CASE(13)
+        TC32_CASE(15)
     default: return cudaErrorInvalidValue;
     }
+#undef TC32_CASE
 }
 
 int hammult_tc32_error(cudaStream_t st)

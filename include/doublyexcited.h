@@ -158,6 +158,22 @@ DE_API int de_set_profiling(de_problem *h, int on);
  * All give the reference's H x to rounding. */
 enum { DE_MATVEC_FMA = 0, DE_MATVEC_TENSOR = 1, DE_MATVEC_STREAM = 2, DE_MATVEC_TF32 = 3 };
 DE_API int de_set_matvec_kernel(de_problem *h, int kind);
+/* The kernels of one matvec pass.  storage 0 = complex128 matvecs, 1 =
+ * complex64 (the mixed form's inner solve); pass 0 = electron-2 axes and
+ * potential, 1 = electron-1 axes; family a DE_MATVEC_* kind (where a
+ * family is not built for the grid, the even/odd kernels run, or the
+ * streaming / cube kernels where those are not built either);
+ * ctas_per_sm caps the resident CTAs per SM of the persistent kernels
+ * (0 = as many as fit).  A handle starts from the tuning table written by
+ * `python -m doublyexcited_b200.tune`: the file DE_MATVEC_TUNING names (set
+ * but empty: none), else matvec_tuning.txt beside the library; entries it
+ * lacks keep the FMA kernels with all resident CTAs.  No reference
+ * counterpart (the reference has one kernel). */
+DE_API int de_set_matvec_launch(de_problem *h, int storage, int pass, int family, int ctas_per_sm);
+DE_API int de_get_matvec_launch(de_problem *h, int storage, int pass, int *family, int *ctas_per_sm);
+/* A tuning table's entry for (storage, NN, pass), read on the host only;
+ * DE_E_INVALID when the file or the entry is missing. */
+DE_API int de_tuning_lookup(const char *path, int storage, int nn, int pass, int *family, int *ctas_per_sm);
 /* Device milliseconds of pass A and pass B, MATBLOCK calls and vectors
  * multiplied since the last read (waits for the recorded events); resets. */
 DE_API int de_profile_read(de_problem *h, double *pass_a_ms, double *pass_b_ms, int64_t *calls,

@@ -191,3 +191,42 @@ def test_server_create_fails_loudly_without_gpu(de):
     with pytest.raises(de.DeError) as e:
         de.Server(workers=2)
     assert e.value.status == de.DE_E_CUDA
+
+
+def test_tuning_table_lookup(de, tmp_path):
+    """The matvec tuning table: entries by storage, grid and pass; comments,
+    malformed lines and unknown families skipped; a missing entry or file
+    reported as such (host only)."""
+    t = tmp_path / "tuning.txt"
+    t.write_text("# storage NN pass family ctas ms\n"
+                 "c64 13 A tf32 2 0.1\n"
+                 "c64 13 B ev 1   # comment\n"
+                 "c128 13 A stream 0 0.2\n"
+                 "c128 13 B bogus 0\n"
+                 "c128 11\n")
+    assert de.tuning_lookup(str(t), "c64", 13, 0) == ("tf32", 2)
+    assert de.tuning_lookup(str(t), "c64", 13, 1) == ("fma", 1)
+    assert de.tuning_lookup(str(t), "c128", 13, 0) == ("stream", 0)
+    assert de.tuning_lookup(str(t), "c128", 13, 1) is None
+    assert de.tuning_lookup(str(t), "c128", 11, 0) is None
+    assert de.tuning_lookup(str(tmp_path / "missing.txt"), "c64", 13, 0) is None
+
+
+def test_committed_tuning_table_covers_the_grids(de):
+    """The committed table (written by python -m doublyexcited_b200.tune on a
+    B200) has an entry for both storages and passes of every grid it
+    tuned, N = 4..9, each a family the grid builds."""
+    import os
+
+    path = os.path.join(os.path.dirname(de.lib_path()), "matvec_tuning.txt")
+    assert os.path.exists(path)
+    for n in range(4, 10):
+        nn = 2 * n + 1
+        for storage in ("c128", "c64"):
+            for pass_ in (0, 1):
+                e = de.tuning_lookup(path, storage, nn, pass_)
+                assert e is not None, (storage, nn, pass_)
+                fam, ctas = e
+                assert fam in ("fma", "tensor", "stream", "tf32") and 0 <= ctas <= 32
+                if fam == "tf32":
+                    assert storage == "c64" and nn <= 15

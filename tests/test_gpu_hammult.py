@@ -296,3 +296,46 @@ def test_tf32_tensor_core_matvec(de, n):
     for j in range(2):
         err = (torch.linalg.norm(y32[j].to(torch.complex128) - y[j]) / torch.linalg.norm(y[j])).item()
         assert err < 1e-6, err
+
+
+def test_handle_reads_the_tuning_table(de):
+    """A handle starts from the committed tuning table's entries."""
+    import os
+
+    path = os.path.join(os.path.dirname(de.lib_path()), "matvec_tuning.txt")
+    with de.Problem(n=6, delta=2.0, theta=0.3, precision="mixed") as g:
+        for storage in ("c128", "c64"):
+            for pass_ in (0, 1):
+                assert g.get_matvec_launch(storage, pass_) == de.tuning_lookup(path, storage, 13, pass_)
+
+
+@pytest.mark.parametrize("n", [4, 6, 7])
+def test_every_tuning_candidate_gives_the_same_matvec(de, n):
+    """Each launch choice the autotuner may pick, on either pass, against the
+    built-in kernels: complex128 within 1e-13, complex64 within 1e-6 of the
+    complex128 result."""
+    import torch
+
+    from doublyexcited_b200.tune import FAMILY_CODE, candidates
+
+    with de.Problem(n=n, delta=2.0, theta=0.3) as g64, \
+            de.Problem(n=n, delta=2.0, theta=0.3, precision="mixed") as g32:
+        st = torch.cuda.current_stream()
+        g64.set_stream(st.cuda_stream)
+        g32.set_stream(st.cuda_stream)
+        gen = torch.Generator(device="cuda").manual_seed(90 + n)
+        x = torch.randn(2, g64.dim, dtype=torch.complex128, device="cuda", generator=gen)
+        ref = torch.empty_like(x)
+        g64.set_matvec_kernel("fma")
+        g64.matblock_d(x.data_ptr(), ref.data_ptr(), 2)
+        x32 = x.to(torch.complex64)
+        for storage, g, xx, tol in (("c128", g64, x, 1e-13), ("c64", g32, x32, 1e-6)):
+            for pass_ in (0, 1):
+                for fam, ctas in candidates(storage, 2 * n + 1):
+                    g.set_matvec_kernel("fma")
+                    g.set_matvec_launch(storage, pass_, FAMILY_CODE[fam], ctas)
+                    y = torch.empty_like(xx)
+                    (g.matblock32_d if storage == "c64" else g.matblock_d)(xx.data_ptr(), y.data_ptr(), 2)
+                    torch.cuda.synchronize()
+                    err = (torch.linalg.norm(y.to(torch.complex128) - ref) / torch.linalg.norm(ref)).item()
+                    assert err < tol, (storage, pass_, fam, ctas, err)
