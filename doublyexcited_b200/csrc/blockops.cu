@@ -772,6 +772,28 @@ __device__ __forceinline__ void raise_flag(int *flag, int bit)
 
 // Upper Cholesky R of the Hermitian G (upper triangle read, as zpotrf 'U')
 // and R^{-1}.  flag |= 1 on breakdown, 2 when G is all zero.
+// Coefficients that orthogonalise one column b against orthonormal columns
+// Q (n of them) and normalise it, from g = [Q^H b; b^H b]: with |w|^2 =
+// b^H b - |Q^H b|^2 (Pythagoras), coef = [-(Q^H b)/|w|; 1/|w|], so that
+// w/|w| = [Q, b] coef.  A |w|^2 not above 1e-28 b^H b raises flag bit 1, as
+// a cholQR breakdown does, and leaves b unchanged.
+__global__ void orth_norm_coef(const double2 *__restrict__ g, int n, double2 *__restrict__ coef, int *flag)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double bb = g[n].x;
+    double w2 = bb;
+    for (int i = 0; i < n; ++i) w2 -= g[i].x * g[i].x + g[i].y * g[i].y;
+    if (!(w2 > 1e-28 * bb)) {
+        raise_flag(flag, 1);
+        for (int i = 0; i < n; ++i) coef[i] = make_double2(0.0, 0.0);
+        coef[n] = make_double2(1.0, 0.0);
+        return;
+    }
+    const double r = 1.0 / sqrt(w2);
+    for (int i = 0; i < n; ++i) coef[i] = make_double2(-g[i].x * r, -g[i].y * r);
+    coef[n] = make_double2(r, 0.0);
+}
+
 __global__ void small_cholinv(const double2 *__restrict__ G, int k, double2 *__restrict__ Rinv, int *flag)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -1707,6 +1729,14 @@ cudaError_t small_sstep_solve_launch(const double2 *g, int nz, double2 *a, int *
 {
     if (nz < 2 || nz > 9) return cudaErrorInvalidValue;
     small_sstep_solve<<<1, 32, 0, st>>>(g, nz, a, flag);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t orth_norm_coef_launch(const double2 *g, int n, double2 *coef, int *flag, cudaStream_t st)
+{
+    if (n < 0 || n > 127) return cudaErrorInvalidValue;
+    orth_norm_coef<<<1, 32, 0, st>>>(g, n, coef, flag);
     count_launch();
     return cudaGetLastError();
 }

@@ -202,6 +202,12 @@ cudaError_t refl_project_launch(double2 *x, int nn, unsigned keep, cudaStream_t 
 cudaError_t to_f32_launch(const double2 *x, float2 *y, int64_t n, cudaStream_t st);
 cudaError_t to_f32_launch(const double *x, float *y, int64_t n, cudaStream_t st);
 
+// Orthogonalise-and-normalise coefficients of one column against n
+// orthonormal columns, from g = [Q^H b; b^H b] (n + 1 entries): coef =
+// [-(Q^H b)/|w|; 1/|w|] with |w|^2 = b^H b - |Q^H b|^2; a |w|^2 not above
+// 1e-28 b^H b raises flag bit 1 (cholQR breakdown).
+cudaError_t orth_norm_coef_launch(const double2 *g, int n, double2 *coef, int *flag, cudaStream_t st);
+
 // k x k (k <= 16) dense helpers that keep the solver on the device.
 // flag bits: 1 Cholesky breakdown, 2 all-zero block, 4 orthonormality
 // self-check failed, 8 singular 1 x 1 Gram.

@@ -78,6 +78,7 @@ struct Solver {
     // conditioning of the k x k Gram (G^-1/2); a gross-failure detector.
     static constexpr double kOrthoTolMixed = 1e-3;
     double2 *dG = nullptr, *dC = nullptr, *dE = nullptr, *dR = nullptr, *dT = nullptr, *dT2 = nullptr;
+    double2 *dOC = nullptr;  // orth_normalize's coefficients
     double2 *dRinv = nullptr, *dGinvh = nullptr, *dGsq = nullptr, *dG1 = nullptr, *dSV = nullptr;
     int *dFlags = nullptr;
     double2 *hbuf = nullptr;  // pinned staging for k x k results (>= 64 x 128 + 64)
@@ -138,6 +139,7 @@ struct Solver {
         DE_TRY(alloc(&dC, 128 * 16));
         DE_TRY(alloc(&dE, 64));
         DE_TRY(alloc(&dR, 64));
+        DE_TRY(alloc(&dOC, 130));
         DE_TRY(alloc(&dT, 64));
         DE_TRY(alloc(&dT2, 65));
         DE_TRY(alloc(&dRinv, 16 * 16));
@@ -308,6 +310,33 @@ struct Solver {
         DE_TRY(gram_dev(L, cols(b, kb, D), dG, L.n));
         DE_TRY(update(xs, clw(b, kb), dG, L.n, -1.0, 1.0));
         if (ab) DE_TRY(update(axs, clw(ab, kb), dG, L.n, -1.0, 1.0));
+        return DE_OK;
+    }
+
+    // One column b: orthogonalised against the union of orthonormal blocks Q
+    // and normalised in one Gram and one update (AB likewise with AQ).  The
+    // Gram also carries b^H b, so |b - Q Q^H b| follows by Pythagoras; the
+    // reference's orthogonalisation followed by cholQR (gplmr.F90:112-196,
+    // lamod.f90:128-180) reads every vector twice more for the same column.
+    int orth_normalize(std::initializer_list<QBlk> qs, double2 *b, double2 *ab = nullptr)
+    {
+        ColList L{};
+        std::vector<const double2 *> xs, axs;
+        for (const QBlk &q : qs)
+            for (int j = 0; j < q.k; ++j) {
+                L.a[L.n++] = col(q.v, j);
+                xs.push_back(col(q.v, j));
+                if (q.av) axs.push_back(col(q.av, j));
+            }
+        const int n = L.n;
+        L.a[L.n++] = b;
+        xs.push_back(b);
+        if (ab) axs.push_back(ab);
+        DE_TRY(gram_dev(L, cols(b, 1, D), dG, L.n));
+        cudaError_t e = orth_norm_coef_launch(dG, n, dOC, dFlags, st);
+        if (e != cudaSuccess) return cuda_error(e, "orth_norm_coef");
+        DE_TRY(update(xs, clw(b, 1), dOC, n + 1, 1.0, 0.0));
+        if (ab) DE_TRY(update(axs, clw(ab, 1), dOC, n + 1, 1.0, 0.0));
         return DE_OK;
     }
 
@@ -985,33 +1014,55 @@ struct Solver {
             fflush(stdout);
         }
         int it = 1;
+        // One column (NEV = 1): X is already unit after normalize(), so its
+        // cholQR is skipped, and each new block is orthogonalised and
+        // normalised in one Gram and one update (orth_normalize).
+        const bool one = nev == 1 && !compat;
         while (it <= maxit && maxres > tol) {
-            DE_TRY(cholqr(X, nev));
-            DE_TRY(trsm(AX, nev));
+            if (!one) {
+                DE_TRY(cholqr(X, nev));
+                DE_TRY(trsm(AX, nev));
+            }
             if (gm.max_inner_iter > 0) DE_TRY(precblock(W, nev));
-            DE_TRY(orth_against(X, nev, W, nev));
-            DE_TRY(cholqr(W, nev));
+            if (one) {
+                DE_TRY(orth_normalize({{X, 1, nullptr}}, W));
+            } else {
+                DE_TRY(orth_against(X, nev, W, nev));
+                DE_TRY(cholqr(W, nev));
+            }
             DE_TRY(matblock(W, AW, nev));
             if (ns > 0) {
                 DE_TRY(minus_e(S, AW, W, nev));
                 if (gm.max_inner_iter > 0) DE_TRY(precblock(S, nev));
-                DE_TRY(orth_against_all({{X, nev, nullptr}, {W, nev, nullptr}}, S, nev));
-                DE_TRY(cholqr(S, nev));
+                if (one) {
+                    DE_TRY(orth_normalize({{X, 1, nullptr}, {W, 1, nullptr}}, S));
+                } else {
+                    DE_TRY(orth_against_all({{X, nev, nullptr}, {W, nev, nullptr}}, S, nev));
+                    DE_TRY(cholqr(S, nev));
+                }
                 DE_TRY(matblock(S, AS, nev));
                 for (int l = 2; l <= ns; ++l) {
                     const int j1 = (l - 1) * nev;
                     double2 *sl = col(S, j1), *asl = col(AS, j1);
                     DE_TRY(minus_e(sl, col(AS, j1 - nev), col(S, j1 - nev), nev));
                     if (gm.max_inner_iter > 0) DE_TRY(precblock(sl, nev));
-                    DE_TRY(orth_against_all({{X, nev, nullptr}, {W, nev, nullptr}, {S, j1, nullptr}}, sl, nev));
-                    DE_TRY(cholqr(sl, nev));
+                    if (one) {
+                        DE_TRY(orth_normalize({{X, 1, nullptr}, {W, 1, nullptr}, {S, j1, nullptr}}, sl));
+                    } else {
+                        DE_TRY(orth_against_all({{X, nev, nullptr}, {W, nev, nullptr}, {S, j1, nullptr}}, sl, nev));
+                        DE_TRY(cholqr(sl, nev));
+                    }
                     DE_TRY(matblock(sl, asl, nev));
                 }
             }
             if (it > 1) {
-                DE_TRY(orth_against_all({{X, nev, AX}, {W, nev, AW}, {S, ldr, AS}}, P, nev, AP));
-                DE_TRY(cholqr(P, nev));
-                DE_TRY(trsm(AP, nev));
+                if (one) {
+                    DE_TRY(orth_normalize({{X, 1, AX}, {W, 1, AW}, {S, ldr, AS}}, P, AP));
+                } else {
+                    DE_TRY(orth_against_all({{X, nev, AX}, {W, nev, AW}, {S, ldr, AS}}, P, nev, AP));
+                    DE_TRY(cholqr(P, nev));
+                    DE_TRY(trsm(AP, nev));
+                }
             }
             // harmonic projection: K = B^H B, M = B^H V, B = A V - sigma V
             const int kdim = (it > 1) ? nproj : nproj - nev;
