@@ -1376,105 +1376,115 @@ namespace {
 // FP64 complex accumulators; every thread has two rows in flight.  Warp
 // shuffles reduce the even and odd lanes separately, then the block, then
 // the last block sums the per-block partials in a fixed order.
-constexpr int kHermNZ = 7, kHermNP = kHermNZ * (kHermNZ + 1) / 2, kHermHalf = kHermNP / 2;
+constexpr int kHermNZ = 7;  // largest power basis (order 6)
 
+// packed index k of the pair (i <= j) of NZ columns, row-major over i
+template <int NZ>
 __host__ __device__ constexpr int herm_i(int k)
 {
     int i = 0;
-    while (k >= kHermNZ - i) {
-        k -= kHermNZ - i;
+    while (k >= NZ - i) {
+        k -= NZ - i;
         ++i;
     }
     return i;
 }
+template <int NZ>
 __host__ __device__ constexpr int herm_j(int k)
 {
     int i = 0;
-    while (k >= kHermNZ - i) {
-        k -= kHermNZ - i;
+    while (k >= NZ - i) {
+        k -= NZ - i;
         ++i;
     }
     return i + k;
 }
 
-// the 14 sums of one half (PART) over two rows
-// the 14 sums of one half (PART) over two rows; K walks them at compile time
-template <int PART, int K>
-__device__ __forceinline__ void herm_acc(double (&ar)[kHermHalf], double (&ai)[kHermHalf], const float2 (&z0)[kHermNZ],
-                                         const float2 (&z1)[kHermNZ])
+// conj(z_i) z_j of one row added to the packed sums; K walks the pairs at
+// compile time.  Products of two floats are exact in double.
+template <int NZ, int K>
+__device__ __forceinline__ void herm_acc(double (&ar)[NZ * (NZ + 1) / 2], double (&ai)[NZ * (NZ + 1) / 2],
+                                         const double (&zr)[NZ], const double (&zi)[NZ])
 {
-    if constexpr (K < kHermHalf) {
-        constexpr int i = herm_i(PART * kHermHalf + K), j = herm_j(PART * kHermHalf + K);
-        // conj(z_i) z_j; products of two floats are exact in double
-        ar[K] = fma((double)z0[i].x, (double)z0[j].x, ar[K]);
-        ar[K] = fma((double)z0[i].y, (double)z0[j].y, ar[K]);
-        ai[K] = fma((double)z0[i].x, (double)z0[j].y, ai[K]);
-        ai[K] = fma(-(double)z0[i].y, (double)z0[j].x, ai[K]);
-        ar[K] = fma((double)z1[i].x, (double)z1[j].x, ar[K]);
-        ar[K] = fma((double)z1[i].y, (double)z1[j].y, ar[K]);
-        ai[K] = fma((double)z1[i].x, (double)z1[j].y, ai[K]);
-        ai[K] = fma(-(double)z1[i].y, (double)z1[j].x, ai[K]);
-        herm_acc<PART, K + 1>(ar, ai, z0, z1);
+    if constexpr (K < NZ * (NZ + 1) / 2) {
+        constexpr int i = herm_i<NZ>(K), j = herm_j<NZ>(K);
+        ar[K] = fma(zr[i], zr[j], ar[K]);
+        ar[K] = fma(zi[i], zi[j], ar[K]);
+        ai[K] = fma(zr[i], zi[j], ai[K]);
+        ai[K] = fma(-zi[i], zr[j], ai[K]);
+        herm_acc<NZ, K + 1>(ar, ai, zr, zi);
     }
 }
 
+// G = Z^H Z (n = NZ complex64 columns, FP64 sums) in one read: each thread
+// adds all NZ (NZ + 1) / 2 packed sums of two rows per step; warps, blocks
+// and the last block's fixed-order tree reduce them.
+template <int NZ>
 __global__ void __launch_bounds__(256, 2)
     gram_herm_kernel(const __grid_constant__ ColListT<float2> Z, int64_t len, double2 *__restrict__ work,
                      double2 *__restrict__ out, int ldo)
 {
-    const int n = Z.n;
+    constexpr int NP = NZ * (NZ + 1) / 2;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int part = warp & 1;  // the two warps of a pair read the same rows
-    double ar[kHermHalf], ai[kHermHalf];
+    double ar[NP], ai[NP];
 #pragma unroll
-    for (int k = 0; k < kHermHalf; ++k) ar[k] = ai[k] = 0.0;
-    const int64_t stride = (int64_t)gridDim.x * (blockDim.x >> 1);
-    const int64_t base = ((int64_t)blockIdx.x * (blockDim.x >> 6) + (warp >> 1)) * 32 + lane;
-    for (int64_t r0 = base; r0 < len; r0 += 2 * stride) {
+    for (int k = 0; k < NP; ++k) ar[k] = ai[k] = 0.0;
+    const float2 *zc[NZ];
+#pragma unroll
+    for (int j = 0; j < NZ; ++j) zc[j] = Z.a[j];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r0 < len; r0 += 2 * stride) {
         const int64_t r1 = r0 + stride;
-        float2 z0[kHermNZ], z1[kHermNZ];
+        const bool has1 = r1 < len;
+        float2 z0[NZ], z1[NZ];
 #pragma unroll
-        for (int j = 0; j < kHermNZ; ++j) {
-            z0[j] = (j < n) ? __ldg(Z.a[j] + r0) : make_float2(0.f, 0.f);
-            z1[j] = (j < n && r1 < len) ? __ldg(Z.a[j] + r1) : make_float2(0.f, 0.f);
+        for (int j = 0; j < NZ; ++j) {
+            z0[j] = __ldg(zc[j] + r0);
+            z1[j] = has1 ? __ldg(zc[j] + r1) : make_float2(0.f, 0.f);
         }
-        if (part == 0) herm_acc<0, 0>(ar, ai, z0, z1);
-        else herm_acc<1, 0>(ar, ai, z0, z1);
-    }
-    // reduce each warp, then the warps of each parity
-    __shared__ double2 wsum[8][kHermHalf];
+        double xr[NZ], xi[NZ];
 #pragma unroll
-    for (int k = 0; k < kHermHalf; ++k) {
+        for (int j = 0; j < NZ; ++j) {
+            xr[j] = z0[j].x;
+            xi[j] = z0[j].y;
+        }
+        herm_acc<NZ, 0>(ar, ai, xr, xi);
+#pragma unroll
+        for (int j = 0; j < NZ; ++j) {
+            xr[j] = z1[j].x;
+            xi[j] = z1[j].y;
+        }
+        herm_acc<NZ, 0>(ar, ai, xr, xi);
+    }
+    __shared__ double2 wsum[8][NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
             ar[k] += __shfl_xor_sync(0xffffffffu, ar[k], off);
             ai[k] += __shfl_xor_sync(0xffffffffu, ai[k], off);
         }
-    }
-    if (lane == 0) {
-#pragma unroll
-        for (int k = 0; k < kHermHalf; ++k) wsum[warp][k] = make_double2(ar[k], ai[k]);
+        if (lane == 0) wsum[warp][k] = make_double2(ar[k], ai[k]);
     }
     __syncthreads();
     unsigned *ticket = reinterpret_cast<unsigned *>(work);
     double2 *part_out = work + 1;
     const int nw = blockDim.x >> 5;
-    if (threadIdx.x < kHermNP) {
-        const int pp = threadIdx.x / kHermHalf, k = threadIdx.x % kHermHalf;
+    if (threadIdx.x < NP) {
         double2 t = make_double2(0.0, 0.0);
-        for (int w = pp; w < nw; w += 2) {
-            t.x += wsum[w][k].x;
-            t.y += wsum[w][k].y;
+        for (int w = 0; w < nw; ++w) {
+            t.x += wsum[w][threadIdx.x].x;
+            t.y += wsum[w][threadIdx.x].y;
         }
-        part_out[(int64_t)blockIdx.x * kHermNP + threadIdx.x] = t;
+        part_out[(int64_t)blockIdx.x * NP + threadIdx.x] = t;
     }
     if (last_block(ticket, gridDim.x)) {
         __shared__ double2 res[32];
-        reduce_partials(part_out, gridDim.x, kHermNP, kHermNP, res);
-        for (int o = threadIdx.x; o < n * n; o += blockDim.x) {
-            const int i = o % n, j = o / n;
+        reduce_partials(part_out, gridDim.x, NP, NP, res);
+        for (int o = threadIdx.x; o < NZ * NZ; o += blockDim.x) {
+            const int i = o % NZ, j = o / NZ;
             const int a = i < j ? i : j, b = i < j ? j : i;
-            const int kk = a * kHermNZ - a * (a - 1) / 2 + (b - a);  // packed index of (a, b)
+            const int kk = a * NZ - a * (a - 1) / 2 + (b - a);  // packed index of (a, b)
             double2 v = res[kk];
             if (i > j) v.y = -v.y;
             out[i + (int64_t)ldo * j] = v;
@@ -1482,18 +1492,32 @@ __global__ void __launch_bounds__(256, 2)
         if (threadIdx.x == 0) *ticket = 0u;
     }
 }
+
+template <int NZ>
+cudaError_t gram_herm_go(const ColListF &Z, int64_t len, double2 *out, int ldo, double2 *work, cudaStream_t st)
+{
+    // partials: NZ (NZ + 1) / 2 per block must fit the reduction scratch (kSmallBlocks * 32)
+    const int64_t want = (len + 511) / 512;
+    const int blocks = (int)std::max<int64_t>(
+        1, std::min<int64_t>(want, std::min(wave_blocks<gram_herm_kernel<NZ>>(), kSmallBlocks)));
+    gram_herm_kernel<NZ><<<blocks, 256, 0, st>>>(Z, len, work, out, ldo);
+    count_launch();
+    return cudaGetLastError();
+}
 }  // namespace
 
 cudaError_t gram_herm_launch(const ColListF &Z, int64_t len, double2 *out, int ldo, double2 *work, cudaStream_t st)
 {
-    if (Z.n < 1 || Z.n > kHermNZ || len < 1) return cudaErrorInvalidValue;
-    // partials: 28 per block must fit the reduction scratch (kSmallBlocks * 32)
-    const int64_t want = (len + 511) / 512;
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min(wave_blocks<gram_herm_kernel>(),
-                                                                                  kSmallBlocks)));
-    gram_herm_kernel<<<blocks, 256, 0, st>>>(Z, len, work, out, ldo);
-    count_launch();
-    return cudaGetLastError();
+    if (len < 1) return cudaErrorInvalidValue;
+    switch (Z.n) {
+    case 2: return gram_herm_go<2>(Z, len, out, ldo, work, st);
+    case 3: return gram_herm_go<3>(Z, len, out, ldo, work, st);
+    case 4: return gram_herm_go<4>(Z, len, out, ldo, work, st);
+    case 5: return gram_herm_go<5>(Z, len, out, ldo, work, st);
+    case 6: return gram_herm_go<6>(Z, len, out, ldo, work, st);
+    case 7: return gram_herm_go<7>(Z, len, out, ldo, work, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 template <class SI, class SO>
