@@ -1182,7 +1182,11 @@ __device__ __forceinline__ void dmma_g(double &d0, double &d1, double a, double 
                  : "d"(a), "d"(b));
 }
 
-template <class S, int MTW, int NTW>
+// KM8: the harmonic projection of one column with a P block (8 x 16): L
+// columns are b_c = a_c - sigma v_c (c < 8) and R is [b_0..b_7, v_0..v_7],
+// so a lane's two loads (a_c, v_c of its column c) give its L fragment and
+// both R fragments.
+template <class S, int MTW, int NTW, bool KM8 = false>
 __global__ void __launch_bounds__(512)
     gram_tc(const __grid_constant__ ColListT<S> L, const __grid_constant__ ColListT<S> R, int64_t len, int64_t chunk,
             int herm, int wm, int wn, int rg, double2 *__restrict__ work)
@@ -1235,12 +1239,21 @@ __global__ void __launch_bounds__(512)
         for (int u = 0; u < US; ++u) {
             const int64_t r = rb + 4 * (int64_t)rg * u + q4;
             const bool rok = r < r1;
+            if constexpr (KM8) {
+                const double2 av = rok ? ld2(la[0] + r) : make_double2(0.0, 0.0);
+                const double2 v = rok ? ld2(lb[0] + r) : make_double2(0.0, 0.0);
+                const double2 sgm = L.sigma;
+                lv[u][0] = make_double2(av.x - (sgm.x * v.x - sgm.y * v.y), av.y - (sgm.x * v.y + sgm.y * v.x));
+                rv[u][0] = lv[u][0];
+                rv[u][1] = v;
+            } else {
 #pragma unroll
-            for (int a = 0; a < MTW; ++a)
-                lv[u][a] = (rok && la[a]) ? elem(la[a], lb[a], L.sigma, r) : make_double2(0.0, 0.0);
+                for (int a = 0; a < MTW; ++a)
+                    lv[u][a] = (rok && la[a]) ? elem(la[a], lb[a], L.sigma, r) : make_double2(0.0, 0.0);
 #pragma unroll
-            for (int b = 0; b < NTW; ++b)
-                rv[u][b] = (rok && ra[b]) ? elem(ra[b], rbp[b], R.sigma, r) : make_double2(0.0, 0.0);
+                for (int b = 0; b < NTW; ++b)
+                    rv[u][b] = (rok && ra[b]) ? elem(ra[b], rbp[b], R.sigma, r) : make_double2(0.0, 0.0);
+            }
         }
 #pragma unroll
         for (int u = 0; u < US; ++u)
@@ -1286,7 +1299,7 @@ __global__ void __launch_bounds__(512)
     }
 }
 
-template <class S, int MTW, int NTW>
+template <class S, int MTW, int NTW, bool KM8 = false>
 static cudaError_t gram_tc_go(const ColListT<S> &L, const ColListT<S> &R, int64_t len, int herm, double2 *out, int ldo,
                               double2 *work, cudaStream_t st)
 {
@@ -1302,7 +1315,7 @@ static cudaError_t gram_tc_go(const ColListT<S> &L, const ColListT<S> &R, int64_
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!attr[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(gram_tc<S, MTW, NTW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(gram_tc<S, MTW, NTW, KM8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              512 * MTW * NTW * 2 * (int)sizeof(double2));
         if (e != cudaSuccess) return e;
         attr[dev] = true;
@@ -1313,7 +1326,7 @@ static cudaError_t gram_tc_go(const ColListT<S> &L, const ColListT<S> &R, int64_
     int64_t chunk = (len + nblk - 1) / nblk;
     chunk = (chunk + 3) / 4 * 4;
     work += 1;
-    gram_tc<S, MTW, NTW><<<nblk, threads, smem, st>>>(L, R, len, chunk, herm, wm, wn, rg, work);
+    gram_tc<S, MTW, NTW, KM8><<<nblk, threads, smem, st>>>(L, R, len, chunk, herm, wm, wn, rg, work);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -1346,6 +1359,12 @@ static cudaError_t gram_any(const ColListT<S> &L, const ColListT<S> &R, int64_t 
     {  // everything else on the FP64 tensor cores
         // warp tiles sized to the output: no more padded tiles than needed
         const int mt = (L.n + 7) / 8, nt = (R.n + 7) / 8;
+        if (L.n == 8 && R.n == 16 && herm) {  // the projection of one column with a P block
+            bool km8 = R.sigma.x == L.sigma.x && R.sigma.y == L.sigma.y;
+            for (int c = 0; c < 8 && km8; ++c)
+                km8 = L.b[c] && R.a[c] == L.a[c] && R.b[c] == L.b[c] && R.a[8 + c] == L.b[c] && !R.b[8 + c];
+            if (km8) return gram_tc_go<S, 1, 2, true>(L, R, len, herm, out, ldo, work, st);
+        }
         if (mt == 1) {
             if (nt == 1) return gram_tc_go<S, 1, 1>(L, R, len, herm, out, ldo, work, st);
             if (nt <= 4) return gram_tc_go<S, 1, 2>(L, R, len, herm, out, ldo, work, st);
