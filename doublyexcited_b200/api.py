@@ -128,8 +128,10 @@ class Problem:
                                          ctypes.byref(c)), "de_get_matvec_launch")
         return self.FAMILIES[f.value], c.value
 
-    def set_profiling(self, on: bool) -> None:
-        check(lib().de_set_profiling(self._h, int(bool(on))), "de_set_profiling")
+    def set_profiling(self, on, every: int = 1) -> None:
+        """Device-time accounting of the matvec passes: off, or on for every
+        `every`-th MATBLOCK call of each storage (1: all of them)."""
+        check(lib().de_set_profiling(self._h, max(1, int(every)) if on else 0), "de_set_profiling")
 
     def profile_read(self) -> dict:
         """Device ms of matvec pass A / pass B, MATBLOCK calls and vectors since

@@ -232,6 +232,7 @@ int de_problem::matblock(const double2 *x, double2 *y, int nvec, double2 shift)
 int de_problem::prof_begin(Rec &r)
 {
     if (!prof) return DE_OK;
+    if (prof_seq[r.f32]++ % prof_every != 0) return DE_OK;  // not sampled: r.e stay null
     for (auto &ev : r.e)
         if (!(ev = take_event())) return set_error(DE_E_CUDA, "cudaEventCreate failed");
     DE_CUDA(cudaEventRecord(r.e[0], stream));
@@ -240,13 +241,13 @@ int de_problem::prof_begin(Rec &r)
 
 int de_problem::prof_mid(Rec &r)
 {
-    if (prof) DE_CUDA(cudaEventRecord(r.e[1], stream));
+    if (prof && r.e[1]) DE_CUDA(cudaEventRecord(r.e[1], stream));
     return DE_OK;
 }
 
 int de_problem::prof_end(Rec &r)
 {
-    if (!prof) return DE_OK;
+    if (!prof || !r.e[2]) return DE_OK;
     DE_CUDA(cudaEventRecord(r.e[2], stream));
     ev_pending.push_back(r);
     if (ev_pending.size() > 4096) DE_TRY(harvest());
@@ -454,7 +455,10 @@ DE_API int de_tuning_lookup(const char *path, int storage, int nn, int pass, int
 DE_API int de_set_profiling(de_problem *h, int on)
 {
     if (!h) return set_error(DE_E_INVALID, "null handle");
+    if (on < 0) return set_error(DE_E_INVALID, "profiling must be 0 (off) or a sampling interval >= 1 (got %d)", on);
     h->prof = on != 0;
+    h->prof_every = on > 1 ? on : 1;
+    h->prof_seq[0] = h->prof_seq[1] = 0;
     return DE_OK;
 }
 

@@ -85,8 +85,11 @@ struct de_problem {
     int64_t work_elems = 0;
     double2 *h_small = nullptr;   // pinned mirror of d_small
     std::mutex mu;
-    // matvec device-time accounting (de_set_profiling)
+    // matvec device-time accounting (de_set_profiling): every prof_every-th
+    // MATBLOCK call of each storage is timed
     bool prof = false;
+    int prof_every = 1;
+    int64_t prof_seq[2] = {0, 0};
     std::vector<cudaEvent_t> ev_free;
     struct Rec {
         cudaEvent_t e[3];

@@ -141,9 +141,13 @@ DE_API int de_problem_dims(const de_problem *h, int *nn, int64_t *m, int64_t *di
 DE_API int de_set_stream(de_problem *h, void *cuda_stream);
 
 /* Device-time accounting of the matvec kernels: CUDA events recorded on the
- * handle's stream around the two passes of every MATBLOCK (pass A: electron-2
- * contraction + potential; pass B: electron-1 contraction).  Off by default.
- * The reference times phases with MPI_WTIME (gplmr.F90:42-57). */
+ * handle's stream around the two passes of MATBLOCK calls (pass A:
+ * electron-2 contraction + potential; pass B: electron-1 contraction).
+ * on = 0: off (the default); 1: every call; n > 1: every n-th call of each
+ * storage (complex128, complex64), which keeps the events' own cost (a few
+ * microseconds a call) out of the timed work; the read-outs then cover the
+ * sampled calls.  The reference times phases with MPI_WTIME
+ * (gplmr.F90:42-57). */
 DE_API int de_set_profiling(de_problem *h, int on);
 /* Which matvec kernels a handle uses: DE_MATVEC_FMA (the default) the
  * fastest CUDA-core kernels per grid: even/odd-split contractions for the
