@@ -230,6 +230,19 @@ __global__ void axpc_kernel(const __grid_constant__ PtrPack P, double2 s, const 
     }
 }
 
+// out = (complex64) (a + s c b) for one column (c = c_dev[0], or 1)
+__global__ void axpc_f32_kernel(float2 *__restrict__ out, const double2 *__restrict__ a,
+                                const double2 *__restrict__ b, double2 s, const double2 *c_dev, int64_t len)
+{
+    const double2 c = c_dev ? c_dev[0] : make_double2(1.0, 0.0);
+    const double2 sc = cmul(s, c);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < len; r += stride) {
+        const double2 av = a[r], bv = b[r];
+        out[r] = make_float2((float)(av.x + sc.x * bv.x - sc.y * bv.y), (float)(av.y + sc.x * bv.y + sc.y * bv.x));
+    }
+}
+
 // out = a + s b over n contiguous elements (FP64 arithmetic, storage S)
 template <class S>
 __global__ void axpy_kernel(S *__restrict__ out, const S *__restrict__ a, const S *__restrict__ b, double2 s,
@@ -961,6 +974,61 @@ __global__ void cvt_r2f_kernel(const double *__restrict__ x, float *__restrict__
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) y[i] = (float)x[i];
 }
 
+// Y = sum_i Z_i a_i (complex64 columns, coefficients on the device) and the
+// exchange projection Y <- (Y + s Y^T)/2 in one pass: a block forms the
+// 32 x 32 tile of Y at (p0, q0) and its transpose partner at (q0, p0) from
+// the inputs, then writes both projected.  Blocks below the diagonal leave
+// at once (their tiles are their partners').
+constexpr int kUxMaxIn = 8;
+struct UxArgs {
+    const float2 *z[kUxMaxIn];
+    int nz;
+};
+
+__global__ void __launch_bounds__(256)
+    update_exch_kernel(const __grid_constant__ UxArgs A, const double2 *__restrict__ coef, double2 *__restrict__ y,
+                       int64_t m, double s)
+{
+    __shared__ double2 ta[32][33], tb[32][33];
+    const int bi = blockIdx.x, bj = blockIdx.y;
+    if (bi > bj) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    const int64_t p0 = (int64_t)bi * 32, q0 = (int64_t)bj * 32;
+    double2 c[kUxMaxIn];
+#pragma unroll
+    for (int i = 0; i < kUxMaxIn; ++i) c[i] = i < A.nz ? coef[i] : make_double2(0.0, 0.0);
+    for (int cc = ty; cc < 32; cc += 8) {
+        // ta[r][cc] = Y(p0 + r, q0 + cc), tb[r][cc] = Y(q0 + r, p0 + cc)
+        const int64_t pa = p0 + tx, qa = q0 + cc, pb = q0 + tx, qb = p0 + cc;
+        const bool oka = pa < m && qa < m, okb = pb < m && qb < m;
+        double ar = 0.0, ai = 0.0, br = 0.0, bim = 0.0;
+#pragma unroll
+        for (int i = 0; i < kUxMaxIn; ++i) {
+            if (i >= A.nz) break;
+            if (oka) {
+                const float2 z = A.z[i][pa + m * qa];
+                ar += (double)z.x * c[i].x - (double)z.y * c[i].y;
+                ai += (double)z.x * c[i].y + (double)z.y * c[i].x;
+            }
+            if (okb) {
+                const float2 z = A.z[i][pb + m * qb];
+                br += (double)z.x * c[i].x - (double)z.y * c[i].y;
+                bim += (double)z.x * c[i].y + (double)z.y * c[i].x;
+            }
+        }
+        ta[tx][cc] = make_double2(ar, ai);
+        tb[tx][cc] = make_double2(br, bim);
+    }
+    __syncthreads();
+    for (int cc = ty; cc < 32; cc += 8) {
+        const int64_t pa = p0 + tx, qa = q0 + cc, pb = q0 + tx, qb = p0 + cc;
+        // Y^T(p, q) = Y(q, p): the partner of ta[r][cc] is tb[cc][r]
+        const double2 a = ta[tx][cc], at = tb[cc][tx], b = tb[tx][cc], bt = ta[cc][tx];
+        if (pa < m && qa < m) y[pa + m * qa] = make_double2(0.5 * (a.x + s * at.x), 0.5 * (a.y + s * at.y));
+        if (bi != bj && pb < m && qb < m) y[pb + m * qb] = make_double2(0.5 * (b.x + s * bt.x), 0.5 * (b.y + s * bt.y));
+    }
+}
+
 int stream_blocks(int64_t len)
 {
     return (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, 148 * 4));
@@ -1581,6 +1649,15 @@ cudaError_t axpc_launch(double2 *const *out, const double2 *const *a, const doub
     return cudaGetLastError();
 }
 
+cudaError_t axpc_f32_launch(float2 *out, const double2 *a, const double2 *b, double2 s, const double2 *c_dev,
+                            int64_t len, cudaStream_t st)
+{
+    if (len < 1) return cudaErrorInvalidValue;
+    axpc_f32_kernel<<<stream_blocks(len) * 2, 256, 0, st>>>(out, a, b, s, c_dev, len);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t axpy_launch(double2 *out, const double2 *a, const double2 *b, double2 s, int64_t n, cudaStream_t st)
 {
     if (n < 1) return cudaErrorInvalidValue;
@@ -1819,6 +1896,19 @@ cudaError_t inv_sqrt_abs_launch(const double2 *d, double2 *c, int n, cudaStream_
 {
     if (n < 1 || n > 64) return cudaErrorInvalidValue;
     inv_sqrt_abs_kernel<<<1, 64, 0, st>>>(d, c, n);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t update_exch_launch(const float2 *const *z, int nz, const double2 *coef, double2 *y, int64_t m, double s,
+                               cudaStream_t st)
+{
+    const int64_t t = (m + 31) / 32;
+    if (m < 1 || t > 65535 || nz < 1 || nz > kUxMaxIn) return cudaErrorInvalidValue;
+    UxArgs A{};
+    for (int i = 0; i < nz; ++i) A.z[i] = z[i];
+    A.nz = nz;
+    update_exch_kernel<<<dim3((unsigned)t, (unsigned)t), 256, 0, st>>>(A, coef, y, m, s);
     count_launch();
     return cudaGetLastError();
 }

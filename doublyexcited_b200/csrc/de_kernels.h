@@ -153,6 +153,9 @@ cudaError_t update_launch(const UpdListT<float2, double2> &U, const double2 *c_d
 // c_dev may be null (c_j = 1).  out may alias a.
 cudaError_t axpc_launch(double2 *const *out, const double2 *const *a, const double2 *const *b,
                         int n, double2 s, const double2 *c_dev, int64_t len, cudaStream_t st);
+// out = (complex64) (a + s c b) for one column, c = c_dev[0] (device) or 1.
+cudaError_t axpc_f32_launch(float2 *out, const double2 *a, const double2 *b, double2 s, const double2 *c_dev,
+                            int64_t len, cudaStream_t st);
 
 // d_j = sum_r conj(A_j[r]) B_j[r] (herm) for j < n (n <= 64) into DEVICE out.
 int64_t dotdiag_work_elems(int n, int64_t len);
@@ -187,6 +190,10 @@ cudaError_t gs_pass2_launch(const float2 *const *qp, const float2 *const *vp, in
 // (Hermitian; work as for gram, >= (M/32)^2 + 1 elements), and the in-place
 // projection X <- (X + s X^T)/2.
 cudaError_t exch_dot_launch(const double2 *x, int64_t m, double2 *out, double2 *work, cudaStream_t st);
+// Y = sum_{i < nz} Z_i coef_i (complex64 columns, nz <= 8, coefficients on
+// the device) written projected, Y <- (Y + s Y^T)/2, in one pass.
+cudaError_t update_exch_launch(const float2 *const *z, int nz, const double2 *coef, double2 *y, int64_t m, double s,
+                               cudaStream_t st);
 cudaError_t exch_project_launch(double2 *x, int64_t m, double s, cudaStream_t st);
 
 // Reflection sectors of one nn^6 vector (nn odd): out[r] = <x, R_r x> for

@@ -74,6 +74,8 @@ struct Solver {
     bool mixed = false;
     double exch_sign = 0.0;     // +1 / -1: exchange symmetry of the start block, 0: none
     unsigned refl_keep = 0xFFu;  // reflection sectors the start block reaches (bit c: sector c)
+    bool exch_done = false;      // the last inner solve's output is already exchange-projected
+    bool z0_staged = false;      // the next inner solve's complex64 start Z_0 is already in Z32
     // The mixed form's self-check: complex64 rounding amplified by the
     // conditioning of the k x k Gram (G^-1/2); a gross-failure detector.
     static constexpr double kOrthoTolMixed = 1e-3;
@@ -390,6 +392,22 @@ struct Solver {
         cudaError_t e = axpc_launch(o.data(), aa.data(), bb.data(), k, make_double2(-1.0, 0.0), dE, D, st);
         if (e != cudaSuccess) return cuda_error(e, "axpc");
         return DE_OK;
+    }
+
+    // S block seed out = AS - S E of the outer iteration (gplmr.F90:147).
+    // When the mixed form's one-column inner solve takes it next, only its
+    // complex64 copy is written, straight into the power basis' Z_0: the
+    // inner solve overwrites out with its result without reading it.
+    int seed(double2 *out, const double2 *a, const double2 *b)
+    {
+        if (nev == 1 && !compat && mixed && order > 1 && order <= 6 && gm.usepetscflag != 0 &&
+            gm.max_inner_iter > 0) {
+            cudaError_t e = axpc_f32_launch(Z32, a, b, make_double2(-1.0, 0.0), dE, D, st);
+            if (e != cudaSuccess) return cuda_error(e, "axpc_f32");
+            z0_staged = true;
+            return DE_OK;
+        }
+        return minus_e(out, a, b, nev);
     }
 
     // E = diag(X^H AX); W = AX - X E; resnrm = sqrt(diag(W^H W)) -> host
@@ -836,10 +854,11 @@ struct Solver {
     int basic_sstep(double2 *b, int k)
     {
         const int nq = order * k, nz = (order + 1) * k;
-        {
+        if (!z0_staged) {
             cudaError_t e = to_f32_launch(b, Z32, (int64_t)k * D, st);
             if (e != cudaSuccess) return cuda_error(e, "to_f32");
         }
+        z0_staged = false;
         for (int i = 1; i <= order; ++i)
             DE_TRY(mult_shifted<float2>(Z32 + (int64_t)(i - 1) * k * D, Z32 + (int64_t)i * k * D, k));
         mv_ref += (order + 1) * k;  // the reference forms (2 order + 1) k products
@@ -850,6 +869,14 @@ struct Solver {
             if (e != cudaSuccess) return cuda_error(e, "gram_herm");
             if ((e = small_sstep_solve_launch(dG, nz, dSV, dFlags, st)) != cudaSuccess)
                 return cuda_error(e, "small_sstep_solve");
+            if (exch_sign != 0.0) {  // the combination and the exchange projection in one pass
+                const float2 *zs[8];
+                for (int i = 0; i < nq; ++i) zs[i] = Z32 + (int64_t)i * D;
+                if ((e = update_exch_launch(zs, nq, dSV, b, h->m, exch_sign, st)) != cudaSuccess)
+                    return cuda_error(e, "update_exch");
+                exch_done = true;
+                return DE_OK;
+            }
             return updateT(Z32, nq, b, 1, dSV, nq);
         }
         std::vector<cplx> g;  // [Z_1..Z_order]^H [Z_0..Z_order], nq x nz
@@ -979,11 +1006,15 @@ struct Solver {
         return DE_OK;
     }
 
-    // Projection of k preconditioned columns onto the start block's sectors.
+    // Projection of k preconditioned columns onto the start block's sectors
+    // (the exchange part skipped when the inner solve's combination already
+    // applied it).
     int symmetry_project(double2 *b, int k)
     {
+        const bool skip_exch = exch_done;
+        exch_done = false;
         for (int j = 0; j < k; ++j) {
-            if (exch_sign != 0.0) {
+            if (exch_sign != 0.0 && !skip_exch) {
                 cudaError_t e = exch_project_launch(col(b, j), h->m, exch_sign, st);
                 if (e != cudaSuccess) return cuda_error(e, "exch_project");
             }
@@ -1032,7 +1063,7 @@ struct Solver {
             }
             DE_TRY(matblock(W, AW, nev));
             if (ns > 0) {
-                DE_TRY(minus_e(S, AW, W, nev));
+                DE_TRY(seed(S, AW, W));
                 if (gm.max_inner_iter > 0) DE_TRY(precblock(S, nev));
                 if (one) {
                     DE_TRY(orth_normalize({{X, 1, nullptr}, {W, 1, nullptr}}, S));
@@ -1044,7 +1075,7 @@ struct Solver {
                 for (int l = 2; l <= ns; ++l) {
                     const int j1 = (l - 1) * nev;
                     double2 *sl = col(S, j1), *asl = col(AS, j1);
-                    DE_TRY(minus_e(sl, col(AS, j1 - nev), col(S, j1 - nev), nev));
+                    DE_TRY(seed(sl, col(AS, j1 - nev), col(S, j1 - nev)));
                     if (gm.max_inner_iter > 0) DE_TRY(precblock(sl, nev));
                     if (one) {
                         DE_TRY(orth_normalize({{X, 1, nullptr}, {W, 1, nullptr}, {S, j1, nullptr}}, sl));
