@@ -985,43 +985,57 @@ struct UxArgs {
     int nz;
 };
 
+template <int NZ>
 __global__ void __launch_bounds__(256)
     update_exch_kernel(const __grid_constant__ UxArgs A, const double2 *__restrict__ coef, double2 *__restrict__ y,
-                       int64_t m, double s)
+                       int64_t m, double s, int t)
 {
     __shared__ double2 ta[32][33], tb[32][33];
-    const int bi = blockIdx.x, bj = blockIdx.y;
-    if (bi > bj) return;
+    // blocks enumerate the tiles on and above the diagonal: bi <= bj
+    int bj = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);
+    while ((bj + 1) * (bj + 2) / 2 <= (int)blockIdx.x) ++bj;
+    while (bj * (bj + 1) / 2 > (int)blockIdx.x) --bj;
+    const int bi = (int)blockIdx.x - bj * (bj + 1) / 2;
+    if (bj >= t) return;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
     const int64_t p0 = (int64_t)bi * 32, q0 = (int64_t)bj * 32;
-    double2 c[kUxMaxIn];
+    double2 c[NZ];
 #pragma unroll
-    for (int i = 0; i < kUxMaxIn; ++i) c[i] = i < A.nz ? coef[i] : make_double2(0.0, 0.0);
-    for (int cc = ty; cc < 32; cc += 8) {
-        // ta[r][cc] = Y(p0 + r, q0 + cc), tb[r][cc] = Y(q0 + r, p0 + cc)
-        const int64_t pa = p0 + tx, qa = q0 + cc, pb = q0 + tx, qb = p0 + cc;
+    for (int i = 0; i < NZ; ++i) c[i] = coef[i];
+    const int64_t pa = p0 + tx, pb = q0 + tx;
+    // every input of the thread's 4 + 4 elements in flight before the sums
+    float2 za[4][NZ], zb[4][NZ];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int cc = ty + 8 * u;
+        const int64_t qa = q0 + cc, qb = p0 + cc;
         const bool oka = pa < m && qa < m, okb = pb < m && qb < m;
+#pragma unroll
+        for (int i = 0; i < NZ; ++i) {
+            za[u][i] = oka ? __ldg(A.z[i] + pa + m * qa) : make_float2(0.f, 0.f);
+            zb[u][i] = okb ? __ldg(A.z[i] + pb + m * qb) : make_float2(0.f, 0.f);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int cc = ty + 8 * u;
         double ar = 0.0, ai = 0.0, br = 0.0, bim = 0.0;
 #pragma unroll
-        for (int i = 0; i < kUxMaxIn; ++i) {
-            if (i >= A.nz) break;
-            if (oka) {
-                const float2 z = A.z[i][pa + m * qa];
-                ar += (double)z.x * c[i].x - (double)z.y * c[i].y;
-                ai += (double)z.x * c[i].y + (double)z.y * c[i].x;
-            }
-            if (okb) {
-                const float2 z = A.z[i][pb + m * qb];
-                br += (double)z.x * c[i].x - (double)z.y * c[i].y;
-                bim += (double)z.x * c[i].y + (double)z.y * c[i].x;
-            }
+        for (int i = 0; i < NZ; ++i) {
+            ar += (double)za[u][i].x * c[i].x - (double)za[u][i].y * c[i].y;
+            ai += (double)za[u][i].x * c[i].y + (double)za[u][i].y * c[i].x;
+            br += (double)zb[u][i].x * c[i].x - (double)zb[u][i].y * c[i].y;
+            bim += (double)zb[u][i].x * c[i].y + (double)zb[u][i].y * c[i].x;
         }
+        // ta[r][cc] = Y(p0 + r, q0 + cc), tb[r][cc] = Y(q0 + r, p0 + cc)
         ta[tx][cc] = make_double2(ar, ai);
         tb[tx][cc] = make_double2(br, bim);
     }
     __syncthreads();
-    for (int cc = ty; cc < 32; cc += 8) {
-        const int64_t pa = p0 + tx, qa = q0 + cc, pb = q0 + tx, qb = p0 + cc;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int cc = ty + 8 * u;
+        const int64_t qa = q0 + cc, qb = p0 + cc;
         // Y^T(p, q) = Y(q, p): the partner of ta[r][cc] is tb[cc][r]
         const double2 a = ta[tx][cc], at = tb[cc][tx], b = tb[tx][cc], bt = ta[cc][tx];
         if (pa < m && qa < m) y[pa + m * qa] = make_double2(0.5 * (a.x + s * at.x), 0.5 * (a.y + s * at.y));
@@ -1904,11 +1918,17 @@ cudaError_t update_exch_launch(const float2 *const *z, int nz, const double2 *co
                                cudaStream_t st)
 {
     const int64_t t = (m + 31) / 32;
-    if (m < 1 || t > 65535 || nz < 1 || nz > kUxMaxIn) return cudaErrorInvalidValue;
+    if (m < 1 || t > 4096 || nz < 1 || nz > kUxMaxIn) return cudaErrorInvalidValue;
     UxArgs A{};
     for (int i = 0; i < nz; ++i) A.z[i] = z[i];
     A.nz = nz;
-    update_exch_kernel<<<dim3((unsigned)t, (unsigned)t), 256, 0, st>>>(A, coef, y, m, s);
+    const unsigned blocks = (unsigned)(t * (t + 1) / 2);
+    switch (nz) {
+#define UX_CASE(K) \
+    case K: update_exch_kernel<K><<<blocks, 256, 0, st>>>(A, coef, y, m, s, (int)t); break;
+        UX_CASE(1) UX_CASE(2) UX_CASE(3) UX_CASE(4) UX_CASE(5) UX_CASE(6) UX_CASE(7) UX_CASE(8)
+#undef UX_CASE
+    }
     count_launch();
     return cudaGetLastError();
 }
