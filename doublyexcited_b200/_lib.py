@@ -201,6 +201,8 @@ SIGNATURES = {
     "de_set_matvec_launch": (INT, [P, INT, INT, INT, INT]),
     "de_get_matvec_launch": (INT, [P, INT, INT, P, P]),
     "de_tuning_lookup": (INT, [ctypes.c_char_p, INT, INT, INT, P, P]),
+    "de_kinetic_precond_d": (INT, [P, P, P, INT, de_complex]),
+    "de_set_gmres_pc": (INT, [P, INT]),
 }
 
 _LIB = None

@@ -169,6 +169,17 @@ class Problem:
         check(lib().de_matblock_d(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), self.m,
                                   self.dim // self.m, nev), "de_matblock_d")
 
+    def kinetic_precond_d(self, x_ptr: int, y_ptr: int, nvec: int, shift: complex = 0.0) -> None:
+        """MSOLVECPLX22 (littlesolver.F90:372-436) on device vectors: the
+        kinetic-eigenbasis preconditioner, y = P x (y must not alias x)."""
+        check(lib().de_kinetic_precond_d(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), nvec,
+                                         de_complex(shift.real, shift.imag)), "de_kinetic_precond_d")
+
+    def set_gmres_pc(self, pcopt: int) -> None:
+        """Preconditioner of the GMRES inner solve (usepetscflag = 0): 0 none
+        (the reference's setting), 2 the kinetic eigenbasis on the left."""
+        check(lib().de_set_gmres_pc(self._h, pcopt), "de_set_gmres_pc")
+
     def matblock32_d(self, x_ptr: int, y_ptr: int, nev: int) -> None:
         """Device-pointer MATBLOCK on complex64 vectors in FP32 arithmetic (the
         mixed form's inner-solve matvec)."""

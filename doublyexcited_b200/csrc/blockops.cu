@@ -1477,8 +1477,6 @@ namespace {
 // FP64 complex accumulators; every thread has two rows in flight.  Warp
 // shuffles reduce the even and odd lanes separately, then the block, then
 // the last block sums the per-block partials in a fixed order.
-constexpr int kHermNZ = 7;  // largest power basis (order 6)
-
 // packed index k of the pair (i <= j) of NZ columns, row-major over i
 template <int NZ>
 __host__ __device__ constexpr int herm_i(int k)

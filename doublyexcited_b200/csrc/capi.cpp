@@ -112,6 +112,45 @@ int de_problem::ensure_stage(int64_t elems)
     return DE_OK;
 }
 
+// MSOLVECPLX22 littlesolver.F90:372-436: W and lam from the real kinetic
+// matrix (KINETIC_EIGS :709-740, here by Jacobi on the host), 1/D for the
+// shift, then the two passes (kinpc.cu).
+int de_problem::kinetic_pc(const double2 *x, double2 *y, int nvec, cplx shift)
+{
+    if (p.nelec != 2) return set_error(DE_E_UNSUPPORTED, "the kinetic preconditioner is built for two electrons");
+    if (!de::kinetic_pc_supported(nn)) return set_error(DE_E_UNSUPPORTED, "kinetic preconditioner: NN %d not built", nn);
+    if (x == y) return set_error(DE_E_INVALID, "kinetic preconditioner: output aliases input");
+    std::vector<double> e, v;
+    if (!d_kw) {
+        de::jacobi_eigen(nn, de::kematrix(nn, delta), e, v);
+        DE_CUDA(cudaMallocAsync(&d_kw, (size_t)nn * nn * sizeof(double), stream));
+        DE_CUDA(cudaMallocAsync(&d_kdinv, (size_t)m * sizeof(double2), stream));
+        DE_CUDA(cudaMemcpyAsync(d_kw, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        DE_CUDA(cudaStreamSynchronize(stream));  // v leaves scope
+        kdinv_ok = false;
+    }
+    if (!kdinv_ok || kdinv_shift != shift) {
+        if (e.empty()) de::jacobi_eigen(nn, de::kematrix(nn, delta), e, v);
+        const cplx scale(ham.sre, ham.sim), s2 = scale * scale;
+        std::vector<double2> d(m);
+        for (int k = 0; k < nn; ++k)
+            for (int j = 0; j < nn; ++j)
+                for (int i = 0; i < nn; ++i) {
+                    const cplx di = 1.0 / ((e[i] + e[j] + e[k]) / s2 - shift);
+                    d[i + (size_t)nn * (j + (size_t)nn * k)] = make_double2(di.real(), di.imag());
+                }
+        DE_CUDA(cudaMemcpyAsync(d_kdinv, d.data(), d.size() * sizeof(double2), cudaMemcpyHostToDevice, stream));
+        DE_CUDA(cudaStreamSynchronize(stream));  // d leaves scope
+        kdinv_shift = shift;
+        kdinv_ok = true;
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+        cudaError_t ce = de::kinetic_pc_launch(nn, x, y, nvec, dim, d_kw, d_kdinv, pass, stream);
+        if (ce != cudaSuccess) return cuda_error(ce, "kinetic preconditioner");
+    }
+    return DE_OK;
+}
+
 int de_problem::ensure_work(int64_t elems)
 {
     if (elems <= work_elems) return DE_OK;
@@ -369,7 +408,7 @@ DE_API int de_problem_destroy(de_problem *h)
     cudaStream_t st = h->own_stream ? h->own_stream : h->stream;
     if (h->stream && h->stream != st) cudaStreamSynchronize(h->stream);
     for (void *p : {(void *)h->d_t1a, (void *)h->d_v12, (void *)h->d_t1af, (void *)h->d_v12f, (void *)h->d_x,
-                    (void *)h->d_y, (void *)h->d_small, (void *)h->d_work})
+                    (void *)h->d_y, (void *)h->d_small, (void *)h->d_work, (void *)h->d_kw, (void *)h->d_kdinv})
         if (p) cudaFreeAsync(p, st);
     for (auto &b : h->cache) cudaFreeAsync(b.p, st);
     cudaStreamSynchronize(st);
@@ -449,6 +488,29 @@ DE_API int de_tuning_lookup(const char *path, int storage, int nn, int pass, int
         return set_error(DE_E_INVALID, "no tuning entry for storage %d, NN %d, pass %d in %s", storage, nn, pass, path);
     *family = f;
     *ctas_per_sm = c;
+    return DE_OK;
+}
+
+DE_API int de_kinetic_precond_d(de_problem *h, const de_complex *x_d, de_complex *y_d, int nvec, de_complex shift)
+{
+    if (!h || !x_d || !y_d) return set_error(DE_E_INVALID, "null argument");
+    if (nvec < 1) return set_error(DE_E_INVALID, "nvec must be >= 1 (got %d)", nvec);
+    std::lock_guard<std::mutex> lk(h->mu);
+    cudaSetDevice(h->p.device);
+    return h->kinetic_pc(reinterpret_cast<const double2 *>(x_d), reinterpret_cast<double2 *>(y_d), nvec,
+                         cplx(shift.re, shift.im));
+}
+
+DE_API int de_set_gmres_pc(de_problem *h, int pcopt)
+{
+    if (!h) return set_error(DE_E_INVALID, "null handle");
+    if (pcopt != 0 && pcopt != 2)
+        return set_error(DE_E_INVALID, "GMRES preconditioner must be 0 (none) or 2 (kinetic eigenbasis), got %d",
+                         pcopt);
+    if (pcopt == 2 && (h->p.nelec != 2 || !de::kinetic_pc_supported(h->nn)))
+        return set_error(DE_E_UNSUPPORTED, "the kinetic preconditioner is built for two electrons at NN 3..19");
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->gm_pcopt = pcopt;
     return DE_OK;
 }
 

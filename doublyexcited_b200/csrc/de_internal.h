@@ -123,4 +123,13 @@ struct de_problem {
     int matblock(const double2 *x, double2 *y, int nvec, double2 shift = double2{0.0, 0.0});
     // the same in FP32 on complex64 vectors (the mixed form's inner solve)
     int matblock32(const float2 *x, float2 *y, int nvec, double2 shift = double2{0.0, 0.0});
+    // the kinetic-eigenbasis preconditioner MSOLVECPLX22 (kinpc.cu), y = P x
+    // on device vectors (y must not alias x); W and 1/D are built on first
+    // use and for each new shift
+    int kinetic_pc(const double2 *x, double2 *y, int nvec, de::cplx shift);
+    int gm_pcopt = 0;  // GMRES inner solve preconditioner: 0 none, 2 kinetic eigenbasis
+    double *d_kw = nullptr;
+    double2 *d_kdinv = nullptr;
+    de::cplx kdinv_shift{0.0, 0.0};
+    bool kdinv_ok = false;
 };

@@ -50,6 +50,15 @@ struct HamDev {
 // Fills ev_ce / ev_co (and the FP32 copies) from h.t for grid h.nn.
 void fill_ev_coefficients(HamDev &h);
 
+// The kinetic-eigenbasis preconditioner MSOLVECPLX22 (kinpc.cu): pass 0
+// writes Y = P on the row cubes, pass 1 adds P on the column cubes; w_dev =
+// W (NN x NN column-major eigenvectors of the real kinetic matrix), dinv_dev
+// = 1 / ((lam_i + lam_j + lam_k) / SCALE^2 - shift) on the cube (M, i
+// fastest).  NN odd, 3..19; y must not alias x.
+bool kinetic_pc_supported(int nn);
+cudaError_t kinetic_pc_launch(int nn, const double2 *x, double2 *y, int nvec, int64_t vstride, const double *w_dev,
+                              const double2 *dinv_dev, int pass, cudaStream_t st);
+
 // Tuning table (tuning.cpp): the entry of (storage 0 complex128 / 1
 // complex64, NN, pass) in the table at path; false when the file or the
 // entry is missing.  apply_tuning fills h.fam / h.ctas for h.nn from the

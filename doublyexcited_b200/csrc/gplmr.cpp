@@ -68,6 +68,9 @@ struct Solver {
     // PETSc-style GMRES inner solve (usepetscflag = 0): basis columns, the
     // iterate and the residual; small device scalars
     static constexpr int kGmresRestart = 30;
+    // GMSOLVER%SHIFT: nothing in the reference assigns it, so its
+    // main-program storage keeps zero
+    const cplx gm_shift{0.0, 0.0};
     double2 *GV = nullptr, *dGs = nullptr;
     float2 *LV32 = nullptr, *LQ32 = nullptr;  // the same in complex64 (unused by the mixed s-step solve)
     float2 *Z32 = nullptr;  // mixed inner solve: the power basis Z_0..Z_order (complex64)
@@ -125,7 +128,7 @@ struct Solver {
             DE_TRY(alloc(&AS, D * ldr));
         }
         if (order > 1 && gm.usepetscflag == 0) {  // GMRES: basis, iterate, residual
-            DE_TRY(alloc(&GV, D * (int64_t)(std::min(order, kGmresRestart) + 3)));
+            DE_TRY(alloc(&GV, D * (int64_t)(std::min(order, kGmresRestart) + 4)));
             DE_TRY(alloc(&dGs, 128));
         } else if (order > 0) {
             const int64_t n = D * (int64_t)std::max(1, order) * nev;
@@ -744,6 +747,8 @@ struct Solver {
     struct GmresDev {
         Solver &S;
         double2 *b, *V, *xg, *r, *dn2, *dy;
+        double2 *out;  // where the solution goes (b is the preconditioned right-hand side when pc)
+        bool pc;       // left preconditioning by MSOLVECPLX22 (GMSOLVER%PCOPT = 2)
 
         int sqnorm_b(double &n2) { return S.sqnorm(b, dn2, &n2); }
         int sqnorm_r(double &n2) { return S.sqnorm(r, dn2, &n2); }
@@ -760,7 +765,12 @@ struct Solver {
         int arnoldi(int k, cplx *coef, double &tt)
         {
             double2 *w = S.col(V, k + 1);
-            DE_TRY(S.matblock(S.col(V, k), w, 1));
+            if (pc) {  // w = M^-1 H v; r is free inside a cycle
+                DE_TRY(S.matblock(S.col(V, k), r, 1));
+                DE_TRY(S.h->kinetic_pc(r, w, 1, S.gm_shift));
+            } else {
+                DE_TRY(S.matblock(S.col(V, k), w, 1));
+            }
             DE_TRY(S.gram_dev(cols(V, k + 1, S.D), cols(w, 1, S.D), S.dGs, k + 1));
             DE_TRY(S.update(S.cl(V, k + 1), {w}, S.dGs, k + 1, -1.0, 1.0));
             const double2 *a[1] = {w};
@@ -785,19 +795,24 @@ struct Solver {
         }
         int zero_result()
         {
-            DE_CUDA(cudaMemsetAsync(b, 0, S.D * sizeof(double2), S.st));
+            DE_CUDA(cudaMemsetAsync(out, 0, S.D * sizeof(double2), S.st));
             return DE_OK;
         }
-        int residual()  // r = b - (H - shift) x, the shift being zero
+        int residual()  // r = b - (H - shift) x (b - M^-1 (H - shift) x when pc), the shift being zero
         {
-            DE_TRY(S.matblock(xg, r, 1));
+            if (pc) {  // the basis is rebuilt from r next: its first column is free
+                DE_TRY(S.matblock(xg, V, 1));
+                DE_TRY(S.h->kinetic_pc(V, r, 1, S.gm_shift));
+            } else {
+                DE_TRY(S.matblock(xg, r, 1));
+            }
             cudaError_t e = axpy_launch(r, b, r, make_double2(-1.0, 0.0), S.D, S.st);
             if (e != cudaSuccess) return cuda_error(e, "axpy");
             return DE_OK;
         }
         int x_to_result()
         {
-            DE_CUDA(cudaMemcpyAsync(b, xg, S.D * sizeof(double2), cudaMemcpyDeviceToDevice, S.st));
+            DE_CUDA(cudaMemcpyAsync(out, xg, S.D * sizeof(double2), cudaMemcpyDeviceToDevice, S.st));
             return DE_OK;
         }
     };
@@ -808,10 +823,25 @@ struct Solver {
     // nothing assigns: its main-program storage is zero, so the operator is H.
     // Each iteration is one matvec, one Gram of the basis against the new
     // vector, one update and one norm, with one host sync for the rotation.
+    //
+    // With the handle's GMRES preconditioner set to 2 (de_set_gmres_pc), the
+    // solve is left-preconditioned by MSOLVECPLX22 -- PETSc's default side
+    // for the shell PC the reference wires as PC_GL = GMSOLVER%PCOPT
+    // (petscsolve.F90:109-114,179) but hard-codes to 0 (input.F90:67):
+    // GMRES on M^-1 (H - shift) x = M^-1 b, the stop test on the
+    // preconditioned residual, with the preconditioner's shift the same
+    // GMSOLVER%SHIFT.
     int gmres_col(double2 *b)
     {
         const int mk = std::min(gm.max_inner_iter, kGmresRestart);
-        GmresDev o{*this, b, GV, GV + (int64_t)(mk + 1) * D, GV + (int64_t)(mk + 2) * D, dGs + 64, dGs + 80};
+        const bool pc = h->gm_pcopt == 2;
+        double2 *rhs = b;
+        if (pc) {  // the preconditioned right-hand side in the spare vector
+            rhs = GV + (int64_t)(mk + 3) * D;
+            DE_TRY(h->kinetic_pc(b, rhs, 1, gm_shift));
+        }
+        GmresDev o{*this, rhs, GV, GV + (int64_t)(mk + 1) * D, GV + (int64_t)(mk + 2) * D, dGs + 64, dGs + 80,
+                   b, pc};
         int its = 0;
         return gmres_run(o, gm.max_inner_iter, gm.tol, kGmresRestart, &its);
     }

@@ -151,6 +151,8 @@ DE_API int de_request_footprint(const de_request *r, int64_t *bytes)
     int64_t vec16 = 6 * nev + 2 * (int64_t)r->ns * nev;
     // inner-solve Krylov blocks LV LQ: complex64 in the mixed form
     int64_t inner_bytes = 2 * order * nev * d * ((p.precision == DE_PREC_MIXED && order > 1) ? 8 : 16);
+    // the GMRES inner solve (usepetscflag = 0) keeps its own basis: restart + 4 vectors
+    if (r->gm.usepetscflag == 0 && order > 1) inner_bytes = (std::min<int64_t>(order, 30) + 4) * d * 16;
     const int64_t work = (1 + std::max<int64_t>(296LL * 64 * 128, 296LL * 32)) * 16;
     const int64_t tables = m * 12 + w * w * w * 12 + 64 * 256 * 16 + 64 * 128 * 16 * 2;
     *bytes = vec16 * d * 16 + inner_bytes + work + tables + (8LL << 20);

@@ -175,6 +175,18 @@ DE_API int de_set_matvec_kernel(de_problem *h, int kind);
  * counterpart (the reference has one kernel). */
 DE_API int de_set_matvec_launch(de_problem *h, int storage, int pass, int family, int ctas_per_sm);
 DE_API int de_get_matvec_launch(de_problem *h, int storage, int pass, int *family, int *ctas_per_sm);
+/* The kinetic-eigenbasis preconditioner MSOLVECPLX22 (littlesolver.F90:
+ * 372-436) on nvec device vectors: with W the eigenvectors and lam the
+ * eigenvalues of the real kinetic matrix (KINETIC_EIGS :709-740) and P = W
+ * diag(1 / ((lam_i + lam_j + lam_k) / SCALE^2 - shift)) W^T on one
+ * electron's cube, y = P on every column cube + P on every row cube.  Two
+ * electrons, NN 3..19; y must not alias x. */
+DE_API int de_kinetic_precond_d(de_problem *h, const de_complex *x_d, de_complex *y_d, int nvec, de_complex shift);
+/* The preconditioner of the GMRES inner solve (de_gmres.usepetscflag = 0):
+ * 0 none (the reference's hard-wired GM_PCOPT, input.F90:67), 2 the
+ * kinetic eigenbasis above applied on the left, as the reference's
+ * PETSc shell PC option 2 would (petscsolve.F90:109-114,179). */
+DE_API int de_set_gmres_pc(de_problem *h, int pcopt);
 /* A tuning table's entry for (storage, NN, pass), read on the host only;
  * DE_E_INVALID when the file or the entry is missing. */
 DE_API int de_tuning_lookup(const char *path, int storage, int nn, int pass, int *family, int *ctas_per_sm);

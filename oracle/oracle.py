@@ -485,6 +485,45 @@ class GmresResult:
     reason: str
 
 
+def kinetic_eigs(h: Hamiltonian) -> tuple[np.ndarray, np.ndarray]:
+    """KINETIC_EIGS littlesolver.F90:709-740: W, the eigenvectors of the real
+    kinetic matrix (DSYEV('V','U') of Re(T)/cos(2 theta), which is T_real),
+    and the eigenvalue sums (lam_i + lam_j + lam_k) / SCALE^2 of the 3D
+    operator on the (NN, NN, NN) grid (i fastest, as ALLEIGS)."""
+    lam, w, info = slapack.dsyev(np.asfortranarray(h.t_real), compute_v=1, lower=0)
+    if info != 0:
+        raise RuntimeError(f"dsyev info {info}")
+    alleigs = (lam[:, None, None] + lam[None, :, None] + lam[None, None, :]) / h.params.scale ** 2
+    return np.asfortranarray(w), alleigs
+
+
+def _axes_apply(x: np.ndarray, mat: np.ndarray, axes) -> np.ndarray:
+    """mat applied along each of the given axes of x: y_a = sum_i mat[a, i] x_i."""
+    for ax in axes:
+        x = np.moveaxis(np.tensordot(mat, x, axes=([1], [ax])), 0, ax)
+    return x
+
+
+def msolve22(h: Hamiltonian, r: np.ndarray, shift: complex = 0.0) -> np.ndarray:
+    """MSOLVECPLX22 littlesolver.F90:372-436, the PETSc path's "spectral
+    decomposition" shell preconditioner (PC option 2).  With W and the
+    eigenvalue sums of kinetic_eigs, P = W diag(1 / (alleigs - shift)) W^T
+    on a 3D cube (EIGMULT hammod.F90:764-799 with WT, the division, EIGMULT
+    with W).  One electron: z = P r.  Two: P on every column cube (electron
+    1) plus P on every row cube (electron 2, through MPITRANSPOSE), added."""
+    nn = h.params.nn
+    w, alleigs = kinetic_eigs(h)
+    dinv = 1.0 / (alleigs - shift)
+    r = np.asarray(r, dtype=np.complex128)
+    if h.nelec == 1:
+        x3 = r.reshape((nn,) * 3, order="F")
+        return _axes_apply(_axes_apply(x3, w.T, (0, 1, 2)) * dinv, w, (0, 1, 2)).reshape(-1, order="F")
+    x6 = r.reshape((nn,) * 6, order="F")  # (i1, j1, k1, i2, j2, k2)
+    z1 = _axes_apply(_axes_apply(x6, w.T, (0, 1, 2)) * dinv[:, :, :, None, None, None], w, (0, 1, 2))
+    z2 = _axes_apply(_axes_apply(x6, w.T, (3, 4, 5)) * dinv[None, None, None, :, :, :], w, (3, 4, 5))
+    return (z1 + z2).reshape(-1, order="F")
+
+
 def petsc_gmres(apply, b: np.ndarray, max_it: int, rtol: float, abstol: float = 1e-50,
                 restart: int = 30, haptol: float = 1e-30) -> GmresResult:
     """KSPSolve as PETSCSOLVE petscsolve.F90:142-279 configures it, called
@@ -571,12 +610,17 @@ def gplmr_eig(h: Hamiltonian, x0: np.ndarray, sigma: complex, ns: int = 5, maxit
               tol: float = 1e-7, order: int = 5, compat_first_column_only: bool = False,
               max_inner_iter: int | None = None, verbose: bool = False, usepetscflag: int = 1,
               gm_tol: float = 1e-3, gm_shift: complex = 0.0, equilibrate: bool = True,
-              symmetry_project: bool = True, mixed: bool = False) -> GplmrResult:
+              symmetry_project: bool = True, mixed: bool = False, gm_pcopt: int = 0) -> GplmrResult:
     """GPLMR_EIG gplmr.F90:9-374 with the BASIC preconditioner, or with
     usepetscflag = 0 the PETSc GMRES one (PRECBLOCK gplmr.F90:466-502):
     GMRES on (H - gm_shift) per column with rtol gm_tol.  The reference's
     GMSOLVER%SHIFT is never assigned and lives in the main program's
-    zero-initialised storage, so gm_shift defaults to 0.
+    zero-initialised storage, so gm_shift defaults to 0.  gm_pcopt = 2
+    preconditions that GMRES on the left with msolve22 (PETSc's default side
+    for a shell PC: GMRES on M^-1 (H - gm_shift) and M^-1 b, the stop test
+    on the preconditioned residual), the option the reference wires as
+    PC_GL = GMSOLVER%PCOPT (petscsolve.F90:109-114,179) but hard-codes to
+    0 (GM_PCOPT, input.F90:67).
 
     equilibrate (default on; off restates the reference exactly): with
     NEV > 1 the residual block handed to PRECBLOCK_BASIC is scaled to unit
@@ -620,8 +664,12 @@ def gplmr_eig(h: Hamiltonian, x0: np.ndarray, sigma: complex, ns: int = 5, maxit
         if usepetscflag == 0:
             out = np.empty_like(blk)
             for j in range(blk.shape[1]):
-                out[:, j] = petsc_gmres(lambda v: h.matvec(v) - gm_shift * v, blk[:, j], max_inner_iter,
-                                        gm_tol).x
+                if gm_pcopt == 2:
+                    out[:, j] = petsc_gmres(lambda v: msolve22(h, h.matvec(v) - gm_shift * v, gm_shift),
+                                            msolve22(h, blk[:, j], gm_shift), max_inner_iter, gm_tol).x
+                else:
+                    out[:, j] = petsc_gmres(lambda v: h.matvec(v) - gm_shift * v, blk[:, j], max_inner_iter,
+                                            gm_tol).x
             return out
 
         def mult(v: np.ndarray) -> np.ndarray:

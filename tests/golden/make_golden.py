@@ -90,7 +90,7 @@ def hammult1_fixture(n, theta, seed):
     return {"n": n, "delta": 2.0, "theta": theta, "seed": seed}, {"x": x, "y": y}
 
 
-def gplmr_fixture(n, theta, sigma, nev, compat, maxit, tol, seed=0, spin="singlet", usepetscflag=1):
+def gplmr_fixture(n, theta, sigma, nev, compat, maxit, tol, seed=0, spin="singlet", usepetscflag=1, gm_pcopt=0):
     p = O.Params(n=n, delta=2.0, theta=theta)
     h = O.init_hamiltonian(p, nelec=2)
     x0 = O.seeded_start(p, nev, seed, spin)
@@ -99,11 +99,12 @@ def gplmr_fixture(n, theta, sigma, nev, compat, maxit, tol, seed=0, spin="single
         "params": {"n": n, "delta": 2.0, "theta": theta, "charge": 2.0},
         "start": {"kind": "seeded_start", "seed": seed, "spin": spin, "nev": nev},
         "solver": {"sigma": _c(sigma), "ns": 5, "order": 5, "maxit": maxit, "tol": tol,
-                   "compat_first_column_only": bool(compat), "usepetscflag": usepetscflag, "gm_tol": 1e-3},
+                   "compat_first_column_only": bool(compat), "usepetscflag": usepetscflag, "gm_tol": 1e-3,
+                   "gm_pcopt": gm_pcopt},
     }
     try:
         r = O.gplmr_eig(h, x0, sigma, ns=5, maxit=maxit, tol=tol, order=5, compat_first_column_only=compat,
-                        usepetscflag=usepetscflag, gm_tol=1e-3)
+                        usepetscflag=usepetscflag, gm_tol=1e-3, gm_pcopt=gm_pcopt)
     except O.OrthoCheckFailed as e:
         # With NEV > 1 the first-column-only product of the reference's
         # allhmultsub is not linear in the block, so harm_orthog_oneblock's
@@ -114,7 +115,8 @@ def gplmr_fixture(n, theta, sigma, nev, compat, maxit, tol, seed=0, spin="single
         "params": {"n": n, "delta": 2.0, "theta": theta, "charge": 2.0},
         "start": {"kind": "seeded_start", "seed": seed, "spin": spin, "nev": nev},
         "solver": {"sigma": _c(sigma), "ns": 5, "order": 5, "maxit": maxit, "tol": tol,
-                   "compat_first_column_only": bool(compat), "usepetscflag": usepetscflag, "gm_tol": 1e-3},
+                   "compat_first_column_only": bool(compat), "usepetscflag": usepetscflag, "gm_tol": 1e-3,
+                   "gm_pcopt": gm_pcopt},
         "iterations": r.iterations,
         "matvecs_reference": r.matvecs,
         "e": [_c(z) for z in r.e],
@@ -247,6 +249,8 @@ FIXTURES = {
                                                                  usepetscflag=0))),
     "gplmr_n3_nev2_petsc": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 2, False, 6, 1e-10,
                                                                  usepetscflag=0))),
+    "gplmr_n3_nev1_petsc_pc2": (True, lambda: ("json", gplmr_fixture(3, 0.3, complex(-0.78, 0), 1, False, 120,
+                                                                     1e-10, usepetscflag=0, gm_pcopt=2))),
     "pipeline_n5_petsc": (True, lambda: ("json", pipeline_n5_petsc())),
     "pipeline_n6_readvecs": (True, lambda: ("json", pipeline_n6_readvecs())),
     "pipeline_n6_readvecs_order20": (True, lambda: ("json", pipeline_n6_readvecs_order20())),

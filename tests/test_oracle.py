@@ -319,3 +319,30 @@ def test_reflection_sectors_are_symmetries_of_h():
     assert O.reflection_sectors(x[:, None], p.nn) == 0xFF
     y = O.reflection_project(x, p.nn, 0x68)
     assert O.reflection_sectors(y[:, None], p.nn) == 0x68
+
+
+def test_kinetic_preconditioner_is_the_3d_kinetic_inverse():
+    """msolve22 (MSOLVECPLX22): for one electron it is (T3/SCALE^2 - s)^-1
+    with T3 the 3D kinetic operator (Kronecker sum of the 1D matrix); for
+    two electrons, that inverse on every column cube plus on every row
+    cube."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    p = O.Params(n=1, delta=2.0, theta=0.3)
+    h1 = O.init_hamiltonian(p, nelec=1)
+    h2 = O.init_hamiltonian(p, nelec=2)
+    nn, m = p.nn, p.m
+    t, e = h1.t_real, np.eye(nn)
+    t3 = (np.kron(np.kron(e, e), t) + np.kron(np.kron(e, t), e) + np.kron(np.kron(t, e), e)) / p.scale ** 2
+    s = complex(-0.4, 0.05)
+    a = np.linalg.inv(t3 - s * np.eye(m))
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(m) + 1j * rng.standard_normal(m)
+    assert np.linalg.norm(O.msolve22(h1, x, s) - a @ x) < 1e-12 * np.linalg.norm(a @ x)
+    xx = rng.standard_normal(m * m) + 1j * rng.standard_normal(m * m)
+    X = xx.reshape((m, m), order="F")
+    ref = a @ X + (a @ X.T).T
+    got = O.msolve22(h2, xx, s).reshape((m, m), order="F")
+    assert np.linalg.norm(got - ref) < 1e-12 * np.linalg.norm(ref)
