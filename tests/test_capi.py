@@ -230,3 +230,18 @@ def test_committed_tuning_table_covers_the_grids(de):
                 assert fam in ("fma", "tensor", "stream", "tf32") and 0 <= ctas <= 32
                 if fam == "tf32":
                     assert storage == "c64" and nn <= 15
+
+
+def test_tuner_candidates_follow_the_built_kernels():
+    """The autotuner times only launch choices the library builds for a
+    grid: even/odd kernels up to NN 13 (complex128) / 17 (complex64), the
+    persistent streaming kernels from NN 13, DMMA on odd NN 9..19, tcgen05
+    TF32 for complex64 up to NN 15; the built-in choice comes first."""
+    from doublyexcited_b200.tune import candidates
+
+    assert candidates("c128", 13)[0] == ("ev", 0) and candidates("c128", 15)[0] == ("stream", 0)
+    assert candidates("c64", 17)[0] == ("ev", 0) and candidates("c64", 19)[0] == ("stream", 0)
+    assert ("tf32", 0) in candidates("c64", 15) and not any(f == "tf32" for f, _ in candidates("c64", 17))
+    assert not any(f == "tf32" for f, _ in candidates("c128", 13))
+    assert ("dmma", 0) in candidates("c128", 19) and not any(f == "dmma" for f, _ in candidates("c128", 7))
+    assert candidates("c128", 7) == [("stream", 0)]

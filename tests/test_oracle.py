@@ -346,3 +346,27 @@ def test_kinetic_preconditioner_is_the_3d_kinetic_inverse():
     ref = a @ X + (a @ X.T).T
     got = O.msolve22(h2, xx, s).reshape((m, m), order="F")
     assert np.linalg.norm(got - ref) < 1e-12 * np.linalg.norm(ref)
+
+
+def test_oracle_mixed_form_keeps_the_start_sectors():
+    """The oracle's restatement of the mixed form (complex64 power basis,
+    symmetry projections) from a singlet start restricted to three
+    reflection sectors, N=2: it converges, its Ritz vector is an eigenvector
+    of H (true residual), and the vector stays in the start's reflection
+    sectors and exchange sector."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    p = O.Params(n=2, delta=2.0, theta=0.3)
+    h = O.init_hamiltonian(p, nelec=2)
+    x = O.reflection_project(O.seeded_start(p, 1, 4, "singlet")[:, 0], p.nn, 0x68)
+    x0 = (x / np.linalg.norm(x))[:, None]
+    r = O.gplmr_eig(h, x0, complex(-0.78, 0), ns=5, maxit=60, tol=1e-10, order=5, mixed=True)
+    assert r.residuals.max() <= 1e-10
+    v = r.x[:, 0] / np.linalg.norm(r.x[:, 0])
+    assert np.linalg.norm(h.matvec(v) - r.e[0] * v) < 1e-9
+    assert O.reflection_sectors(v[:, None], p.nn) == 0x68
+    m = p.m
+    z = v.reshape(m, m, order="F")
+    assert np.linalg.norm(z - z.T) < 1e-6 * np.linalg.norm(z)
