@@ -165,9 +165,9 @@ def alg_bytes(nn):
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, pass A + pass B)
 # per vector-matvec of the kernels the library picks, keyed by (NN,
 # storage): one ncu capture of the block-of-2 matvec at N=6 (`--workload
-# matvec-n6`), both passes' bytes over 2 vectors: ev_kernel<float, 13>.
-# Kernels without a capture report null.
-NCU_TRAFFIC_PER_VECTOR = {(13, "f32"): 149.4e6}
+# matvec-n6`), both passes' bytes over 2 vectors: ev_kernel<float, 13> and
+# ev_kernel<double, 13>.  Kernels without a capture report null.
+NCU_TRAFFIC_PER_VECTOR = {(13, "f32"): 149.3e6, (13, "f64"): 342.6e6}
 
 # The timed solves keep the library's matvec events on for the roofline
 # figures, on every 8th MATBLOCK call of each storage: all calls of one
