@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <mutex>
 
 namespace de {
@@ -29,6 +30,14 @@ namespace de {
 static std::atomic<int64_t> g_launches{0};
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 int64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+bool programmatic_launch()
+{
+    static const bool on = [] {
+        const char *v = std::getenv("DE_PDL");
+        return !(v && v[0] == '0' && v[1] == 0);
+    }();
+    return on;
+}
 
 namespace {
 

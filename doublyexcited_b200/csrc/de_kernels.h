@@ -11,6 +11,10 @@ namespace de {
 // Process-wide count of kernels launched by this library.
 void count_launch(int n = 1);
 int64_t launch_count();
+// Whether the even/odd matvec kernels are launched as programmatic dependent
+// launches (they wait on the grid dependency after their table preload);
+// on unless the environment sets DE_PDL=0.  Read once per process.
+bool programmatic_launch();
 
 constexpr int kMaxNN = 27;      // N <= 13 (the reference ran N = 5..15)
 constexpr int kEvCoef = 12 * 12;  // even/odd coefficient tables, N <= 11

@@ -558,6 +558,12 @@ __global__ void __launch_bounds__(EvCfg<R, NN, MODE>::T, EvShape<R, NN, MODE>::M
         const R *t1a = t1a_of<R>(h);
         for (int e = o; e < C::M; e += C::T) t1as[e] = __ldg(t1a + e);
     }
+    // Programmatic dependent launch: everything above reads only the
+    // operator's tables, written once at set-up.  X and Y are touched after
+    // the stream's previous kernel has completed and its writes are visible
+    // (a no-op when the launch carries no programmatic attribute).  Every CTA
+    // waits, so this grid never completes before its predecessor.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     UnitView<R> cur;
     cur.valid = false;
     if (nloc > 0) {
@@ -571,6 +577,9 @@ __global__ void __launch_bounds__(EvCfg<R, NN, MODE>::T, EvShape<R, NN, MODE>::M
     const R sc2r = (R)(h.sre * h.sre - h.sim * h.sim), sc2i = (R)(2.0 * h.sre * h.sim);
     for (int64_t ul = 0; ul < nloc; ++ul) {
         const int64_t unext = ul + 1 < nloc ? blockIdx.x + (ul + 1) * gridDim.x : -1;
+        // the last unit: let the stream's next programmatic launch be
+        // scheduled (it waits for this grid's completion before reading)
+        if (unext < 0) asm volatile("griddepcontrol.launch_dependents;");
         Acc<R, NN> A;
 #pragma unroll
         for (int q = 0; q <= N; ++q) A.er[q] = A.ei[q] = A.orr[q] = A.oi[q] = R(0);
@@ -650,8 +659,19 @@ cudaError_t ev_launch(const HamDev &h, const CX<R> *x, CX<R> *y, int nvec, int64
     a.upv = MODE == 0 ? (C::M + C::PB - 1) / C::PB : C::M;
     a.nunits = (int64_t)a.upv * nvec;
     const int64_t grid = std::min<int64_t>(a.nunits, (int64_t)ev_sm_count() * per_sm);
-    ev_kernel<R, NN, MODE><<<(unsigned)grid, C::T, C::SMEM, st>>>(h, a);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(C::T);
+    cfg.dynamicSmemBytes = C::SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = programmatic_launch() ? 1 : 0;
+    e = cudaLaunchKernelEx(&cfg, ev_kernel<R, NN, MODE>, h, a);
     count_launch();
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
