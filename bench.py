@@ -19,10 +19,11 @@ reports both rates and |dE| between them.
          matvec in the plain form; two passes per vector), timed with CUDA
          events recorded by the library on its stream over the timed region;
          the other matvec is reported beside it
-  cpu_baseline  the oracle's HAMMULT (the reference's KEMULT2 loop structure
-         in C with OpenMP, all host cores) on a bounded sample of matvecs,
-         converted with the solve's HAMMULT count; block operations are not
-         charged, so it is a lower bound on the CPU solve time
+  cpu_baseline  the oracle (the reference's loops restated: HAMMULT in C
+         with OpenMP on all host cores, the inner solve and block operations
+         in numpy/LAPACK) timed on a bounded sample, a few preconditioned
+         blocks of one GPLMR iteration, and scaled by the blocks per
+         iteration and the iterations the GPU solve took
 
 Other workloads: ``matvec-n9`` / ``matvec-n8`` / ``matvec-n6`` (one step =
 H applied to a block of vectors, FP64 and FP32 with the relative error per
@@ -139,6 +140,7 @@ def run_served(de, seeded_start, cfg, precision, workers=None):
             "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "ok": int(sum(ok)),
             "converged": int(sum(conv)), "e": {i: done[i].e.copy() for i in range(len(reqs))},
             "conv": {i: bool(done[i].converged and done[i].status == 0) for i in range(len(reqs))},
+            "iters": {i: int(done[i].iterations) for i in range(len(reqs))},
             "not_converged": [dict(reqs[i], status=int(done[i].status)) for i in range(len(reqs))
                               if not (done[i].converged and done[i].status == 0)]}
 
@@ -362,6 +364,29 @@ class OracleBlockStep:
         return time.perf_counter() - t0
 
 
+def serve_cpu_baseline(cfg, reqs, iters, ns=5):
+    """The oracle on a served or batched mix, one solve at a time on all
+    host cores (the reference runs one solve per job).  One preconditioned
+    block with one column (OracleBlockStep) is timed per grid size N of the
+    mix; each request is charged that time x its NEV (the block's matvecs,
+    inner solve and projections grow with the columns) x (1 + NS) blocks
+    per iteration (gplmr.F90:92-190) x the iterations its GPU solve took."""
+    t_blk = {}
+    for n in sorted({r["n"] for r in reqs}):
+        w = dict(n=n, delta=2.0, theta=cfg["thetas"][0], nev=1, seed=0, spin="singlet", order=5,
+                 sigma=cfg["sigma"], ns=ns)
+        t_blk[n] = OracleBlockStep(w).seconds()
+    cpu_s = sum(t_blk[r["n"]] * r["nev"] * (1 + ns) * max(1, iters[i]) for i, r in enumerate(reqs))
+    cores = os.cpu_count()
+    blocks = ", ".join(f"N={n} {t:.3f} s" for n, t in t_blk.items())
+    return {"value": len(reqs) / cpu_s, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"one preconditioned one-column block of the oracle per grid size ({blocks}: "
+                      f"PRECBLOCK_BASIC, projection, cholQR, MATBLOCK; C HAMMULT with OpenMP on {cores} "
+                      f"threads, block operations in numpy/LAPACK) x NEV x {1 + ns} blocks per iteration "
+                      f"x each request's GPU iteration count, summed over the {len(reqs)} requests "
+                      f"(one solve at a time)"}
+
+
 def run_reference(a, w):
     """--impl reference: the reference's CPU path (the oracle restatement: the
     Fortran/MPI/PETSc program cannot be built on this image) on the same
@@ -566,10 +591,11 @@ def serve_main(a):
     plain = run_served(de, seeded_start, cfg, "fp64", workers=1)
     # the mixed solver one solve at a time (what concurrency adds)
     mixed1 = run_served(de, seeded_start, cfg, "mixed", workers=1) if a.workload == "batch" else None
+    cpu = None if a.no_cpu_baseline else serve_cpu_baseline(cfg, serve_requests(cfg), mixed["iters"])
     both = [i for i in mixed["e"] if mixed["conv"][i] and fp64["conv"][i]]
     de_max = max((float(np.max(np.abs(np.sort_complex(mixed["e"][i]) - np.sort_complex(fp64["e"][i]))))
                   for i in both), default=None)
-    strip = lambda d: {k: v for k, v in d.items() if k not in ("e", "conv")}  # noqa: E731
+    strip = lambda d: {k: v for k, v in d.items() if k not in ("e", "conv", "iters")}  # noqa: E731
     name = "batched uneven solves" if a.workload == "batch" else "served stream"
     line = {"metric": f"resonance solves/s ({name})", "value": mixed["solves_per_s"], "unit": "solves/s",
             "n_gpus": 1, "steps": cfg["requests"], "warmup": 2 * len(cfg["ns"]), "ms_per_step": mixed["wall_s"] / cfg["requests"] * 1e3,
@@ -585,6 +611,7 @@ def serve_main(a):
             "speedup_vs_plain_fp64_solver": mixed["solves_per_s"] / plain["solves_per_s"],
             "dE_mixed_vs_fp64_max": de_max,
             "dE_compared": len(both),
+            "cpu_baseline": cpu,
             "gpu_launches": int(launches), "clocks": clocks}
     print(json.dumps(line))
     return 0
