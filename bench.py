@@ -27,8 +27,11 @@ reports both rates and |dE| between them.
 
 Other workloads: ``matvec-n9`` / ``matvec-n8`` / ``matvec-n6`` (one step =
 H applied to a block of vectors, FP64 and FP32 with the relative error per
-call, CUDA-core and tensor-core kernels), and ``serve`` (a seeded Poisson
-stream of uneven solve requests through the server: solves/s, p50/p99).
+call, CUDA-core and tensor-core kernels), ``serve`` (a seeded Poisson
+stream of uneven solve requests through the server: solves/s, p50/p99) and
+``batch`` (64 uneven requests queued at once).  Their roofline is the
+stream's matvec flops over its wall time, a lower bound; their CPU
+baseline charges each request oracle block times for its grid.
 
 ``--impl reference`` runs that CPU path alone (rank 0) and prints its line.
 Multi-GPU: independent replicas (one solve stream per rank, no collective
@@ -141,6 +144,7 @@ def run_served(de, seeded_start, cfg, precision, workers=None):
             "converged": int(sum(conv)), "e": {i: done[i].e.copy() for i in range(len(reqs))},
             "conv": {i: bool(done[i].converged and done[i].status == 0) for i in range(len(reqs))},
             "iters": {i: int(done[i].iterations) for i in range(len(reqs))},
+            "matvecs": {i: int(done[i].matvecs) for i in range(len(reqs))},
             "not_converged": [dict(reqs[i], status=int(done[i].status)) for i in range(len(reqs))
                               if not (done[i].converged and done[i].status == 0)]}
 
@@ -362,6 +366,21 @@ class OracleBlockStep:
         O.cholqr(b)
         self.h.matblock(b)
         return time.perf_counter() - t0
+
+
+def serve_roofline(reqs, matvecs, wall_s, peak_tflops):
+    """The served or batched stream's matvec work rate: the algorithmic
+    flops of every vector-matvec of every request (alg_flops at its grid)
+    over the stream's wall time.  The wall time also holds everything that
+    is not a matvec, so this is a lower bound on the matvec kernels' own
+    rate; the denominator is the measured FP32 peak, as for the mixed
+    form's matvec."""
+    flops = sum(matvecs[i] * alg_flops(2 * r["n"] + 1) for i, r in enumerate(reqs))
+    achieved = flops / wall_s / 1e12
+    return {"bound": "fp32-fma", "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
+            "frac": achieved / peak_tflops, "traffic": None,
+            "kernel": "all vector-matvecs of the stream (both precisions) over its wall time: a lower bound",
+            "matvecs": int(sum(matvecs.values())), "alg_flops": float(flops), "wall_s": wall_s}
 
 
 def serve_cpu_baseline(cfg, reqs, iters, ns=5):
@@ -591,11 +610,13 @@ def serve_main(a):
     plain = run_served(de, seeded_start, cfg, "fp64", workers=1)
     # the mixed solver one solve at a time (what concurrency adds)
     mixed1 = run_served(de, seeded_start, cfg, "mixed", workers=1) if a.workload == "batch" else None
-    cpu = None if a.no_cpu_baseline else serve_cpu_baseline(cfg, serve_requests(cfg), mixed["iters"])
+    reqs = serve_requests(cfg)
+    roofline = serve_roofline(reqs, mixed["matvecs"], mixed["wall_s"], fp32_peak_tflops(torch))
+    cpu = None if a.no_cpu_baseline else serve_cpu_baseline(cfg, reqs, mixed["iters"])
     both = [i for i in mixed["e"] if mixed["conv"][i] and fp64["conv"][i]]
     de_max = max((float(np.max(np.abs(np.sort_complex(mixed["e"][i]) - np.sort_complex(fp64["e"][i]))))
                   for i in both), default=None)
-    strip = lambda d: {k: v for k, v in d.items() if k not in ("e", "conv", "iters")}  # noqa: E731
+    strip = lambda d: {k: v for k, v in d.items() if k not in ("e", "conv", "iters", "matvecs")}  # noqa: E731
     name = "batched uneven solves" if a.workload == "batch" else "served stream"
     line = {"metric": f"resonance solves/s ({name})", "value": mixed["solves_per_s"], "unit": "solves/s",
             "n_gpus": 1, "steps": cfg["requests"], "warmup": 2 * len(cfg["ns"]), "ms_per_step": mixed["wall_s"] / cfg["requests"] * 1e3,
@@ -611,6 +632,7 @@ def serve_main(a):
             "speedup_vs_plain_fp64_solver": mixed["solves_per_s"] / plain["solves_per_s"],
             "dE_mixed_vs_fp64_max": de_max,
             "dE_compared": len(both),
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches), "clocks": clocks}
     print(json.dumps(line))

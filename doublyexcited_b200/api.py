@@ -361,6 +361,7 @@ class ServedResult:
     footprint_bytes: int
     worker: int
     tag: object = None
+    matvecs: int = 0  # vector-matvecs of the solve, both precisions (de_stats.matvecs)
 
     @property
     def latency_s(self) -> float:
@@ -416,7 +417,8 @@ class Server:
         r, x, e, tag = self._live.pop(res.id)
         st = res.stats
         return ServedResult(res.id, res.status, e, x, st.iterations, bool(st.converged), st.max_residual,
-                            res.t_submit_s, res.t_start_s, res.t_end_s, res.footprint_bytes, res.worker, tag)
+                            res.t_submit_s, res.t_start_s, res.t_end_s, res.footprint_bytes, res.worker, tag,
+                            matvecs=int(st.matvecs))
 
     def wait(self, rid: int, timeout_s: float = -1.0) -> ServedResult:
         res = _l.de_result()

@@ -32,3 +32,12 @@ def test_serve_cpu_baseline_runs_the_oracle():
     out = bench.serve_cpu_baseline(CFG, [dict(n=2, nev=1), dict(n=2, nev=2)], {0: 2, 1: 2})
     assert out["value"] > 0 and math.isfinite(out["value"])
     assert "N=2" in out["sample"] and "2 requests" in out["sample"]
+
+
+def test_serve_roofline_is_the_streams_matvec_rate():
+    reqs = [dict(n=3, nev=1), dict(n=4, nev=2)]
+    out = bench.serve_roofline(reqs, {0: 100, 1: 40}, 2.0, 50.0)
+    flops = 100 * bench.alg_flops(7) + 40 * bench.alg_flops(9)
+    assert math.isclose(out["achieved"], flops / 2.0 / 1e12, rel_tol=1e-12)
+    assert math.isclose(out["frac"], out["achieved"] / 50.0, rel_tol=1e-12)
+    assert out["matvecs"] == 140 and out["unit"] == "TFLOP/s" and out["traffic"] is None

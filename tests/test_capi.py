@@ -193,6 +193,21 @@ def test_server_create_fails_loudly_without_gpu(de):
     assert e.value.status == de.DE_E_CUDA
 
 
+def test_server_result_carries_the_solve_stats(de):
+    # the de_result -> ServedResult conversion, on a result struct filled here
+    from doublyexcited_b200 import _lib as L
+
+    srv = object.__new__(de.Server)  # no device: only the bookkeeping of collected requests
+    x, e = np.zeros((4, 1), np.complex128), np.zeros(1, np.complex128)
+    srv._live = {7: (None, x, e, "tag-7")}
+    res = L.de_result(id=7, status=0, t_submit_s=1.0, t_start_s=1.5, t_end_s=4.0, footprint_bytes=123, worker=2)
+    res.stats.iterations, res.stats.converged, res.stats.matvecs, res.stats.max_residual = 12, 1, 433, 5e-9
+    r = srv._result(res)
+    assert (r.id, r.status, r.iterations, r.converged, r.matvecs, r.worker, r.tag) == (7, 0, 12, True, 433, 2, "tag-7")
+    assert r.x is x and r.e is e and r.latency_s == 3.0 and r.footprint_bytes == 123
+    assert not srv._live
+
+
 def test_tuning_table_lookup(de, tmp_path):
     """The matvec tuning table: entries by storage, grid and pass; comments,
     malformed lines and unknown families skipped; a missing entry or file
